@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark of MARL's per-tick field-and-cell path on B200.
+
+Workload: the reference default run — 128x128x64 grid, 12 external species,
+Winogradsky boundary priming, 3 x 30 seeded starter cells, host RNG seed 42,
+10 diffusion substeps per tick, f32.  One step = one tick of marl_sim::run's
+loop: boundary sources, diffusion, light, the sequential cell loop (device),
+then the change list to the host, fate/division/mutation on the host, and the
+edit list back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Printed (rank 0, one JSON line):
+  value       ticks/s with all state resident in HBM: K ticks / summed device
+              time of the ticks (CUDA events on the engine's stream around the
+              tick kernels + change-list copy and around the edit copy +
+              kernels); the host fate step between them is excluded here.
+  e2e         ticks/s through the public C-ABI engine call (marl_engine_step):
+              wall time of the whole tick including the device->host change
+              list, the host fate step and the host->device edit list.
+  roofline    the dominant kernel (diffusion substep): algorithmic bytes
+              (97 B/voxel: 48 read + 48 written + 1 mask) / CUDA-event time.
+  cpu_baseline  the CPU oracle (restatement of the reference) on this host.
+Multi-GPU: independent replicas (one run per GPU, no collective on the data
+path); value = total ticks of all ranks / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "marl-ochre_b200"))
+
+DIMS = (128, 128, 64)
+SEED = 42
+SEED_COUNT = 30
+METRIC = "ticks/s at 128x128x64 (plain vs batched/surrogate, <=1e-3 rel err); HBM GB/s"
+BYTES_PER_VOXEL_SUBSTEP = 97  # 48 B read + 48 B written + 1 B occupancy
+L2_FLUSH_BYTES = 256 << 20
+REFERENCE_TICKS_PER_S = 1.9  # reference CPU engine, 128x128x64 (recorded in the reference's notes)
+WORKLOAD = ("reference default run: 128x128x64 grid, 12 species, Winogradsky boundary priming, "
+            "3 starters x 30 seeded cells, host RNG seed 42, 10 diffusion substeps/tick, f32")
+
+
+def peaks() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(name: str):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed loop runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(budget_s: float = 15.0, max_ticks: int = 60) -> dict:
+    """The CPU oracle (restatement of the reference) on the same workload, this host's cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    w = oracle.World(DIMS, seed=SEED, seed_count=SEED_COUNT)
+    w.tick(1)  # warm-up (page-in, thread pool)
+    n, t0 = 0, time.perf_counter()
+    while n < max_ticks and time.perf_counter() - t0 < budget_s:
+        w.tick(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "ticks/s", "cores": threads, "kind": "port",
+            "sample": f"{n} ticks (ticks 1..{n}) of the same seed-42 default run; diffusion over z on "
+                      f"{threads} OpenMP threads as rayon does, light and cells single-threaded"}
+
+
+def run_reference(args) -> int:
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    w = oracle.World(DIMS, seed=SEED, seed_count=SEED_COUNT)
+    w.tick(max(args.warmup, 0))
+    budget = 120.0
+    n, t0 = 0, time.perf_counter()
+    while n < args.steps and time.perf_counter() - t0 < budget:
+        w.tick(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    v = n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ticks/s", "n_gpus": args.gpus, "steps": n,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * dt / max(n, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": v / REFERENCE_TICKS_PER_S, "dtype": "f32",
+        "data": "synthetic (seeded Winogradsky initial condition)",
+        "config": {"workload": WORKLOAD, "grid": list(DIMS), "seed": SEED, "seed_count": SEED_COUNT},
+        "cpu_baseline": {"value": v, "unit": "ticks/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} ticks after {args.warmup} warm-up ticks (at most {budget:.0f} s); CPU "
+                                   f"restatement of the reference (the Rust engine cannot be built here)"},
+        "e2e": {"value": v, "unit": "ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def diffusion_roofline(marl, torch, engine, stream) -> dict:
+    """Times the diffusion substep on the engine's current state with CUDA events."""
+    ctx = marl.Context(DIMS, engine.params, cell_capacity=max(int(engine.stats()["population"]), 1) + 16)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_field(engine.field())
+    ctx.upload_cells(engine.cells())
+    us = ctx.autotune(5)
+    tile, zc = ctx.get_tile()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    groups, per_group = 20, 10
+    for _ in range(3):
+        ctx.diffuse(per_group)
+    total_ms = 0.0
+    for _ in range(groups):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.diffuse(per_group)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    t_sub = total_ms / 1000.0 / (groups * per_group)
+    V = DIMS[0] * DIMS[1] * DIMS[2]
+    bytes_per_launch = BYTES_PER_VOXEL_SUBSTEP * V
+    achieved = bytes_per_launch / t_sub / 1e9
+    peak, src = peaks()
+    traffic = ncu_traffic("diffusion_traffic.json")
+    tr = None
+    if traffic and traffic.get("grid") == list(DIMS):
+        tr = traffic.get("dram_bytes_per_launch")
+    ctx.close()
+    tiles = ["32x8", "32x4", "64x4", "16x16"]
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": tr, "kernel": "k_diffuse (diffusion substep, TMA z-march)", "peak_source": src,
+            "algorithmic_bytes_per_launch": bytes_per_launch, "us_per_launch": t_sub * 1e6,
+            "tile": f"{tiles[tile]} columns, z-chunk {zc}", "autotune_us_per_substep": us,
+            "l2": "flushed between groups of 10 substeps (one tick's worth)"}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import marl_cuda as marl
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+
+    eng = marl.Engine(DIMS, marl.default_params(), rng_seed=SEED, seed_count=SEED_COUNT, cell_capacity=1 << 20)
+    eng.set_stream(stream.cuda_stream)
+    eng.autotune(5)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    eng.step(args.warmup)
+    pop0 = eng.stats()["population"]
+
+    sampler = ClockSampler(torch.cuda.current_device())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    c0 = eng.counters()
+    sampler.start()
+    wall = 0.0
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between steps (outside the timed spans)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.step(1)
+        torch.cuda.synchronize()
+        wall += time.perf_counter() - t0
+        s = eng.stats()
+        h2d += s["h2d_bytes_last_tick"]
+        d2h += s["d2h_bytes_last_tick"]
+    torch.cuda.synchronize()
+    c1 = eng.counters()
+    clocks = sampler.stop()
+    dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
+    launches = c1["kernel_launches"] - c0["kernel_launches"]
+    st = eng.stats()
+    if dist:
+        t = torch.tensor([dev_s, wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, wall = float(t[0]), float(t[1])
+        dist.barrier()
+    total_ticks = args.steps * world
+    value = total_ticks / dev_s
+    e2e = total_ticks / wall
+
+    roof = diffusion_roofline(marl, torch, eng, stream) if rank == 0 else None
+    if rank == 0:
+        base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline()
+        line = {
+            "metric": METRIC, "value": value, "unit": "ticks/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": value / REFERENCE_TICKS_PER_S, "dtype": "f32",
+            "data": "synthetic (seeded Winogradsky initial condition of the reference default run)",
+            "config": {"workload": WORKLOAD, "grid": list(DIMS), "seed": SEED, "seed_count": SEED_COUNT,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed between steps (256 MiB device write, outside the timed spans)",
+                       "population_start": int(pop0), "population_end": int(st["population"]),
+                       "divisions": int(st["total_divisions"]), "deaths": int(st["total_deaths"])},
+            "roofline": roof,
+            "cpu_baseline": base,
+            "e2e": {"value": e2e, "unit": "ticks/s", "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": d2h / args.steps,
+                    "api": "marl_engine_step (C ABI), wall clock per tick"},
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,349 @@
+/*
+ * marl_cuda.h — C ABI of libmarl_cuda.so, the sm_100a backend for MARL's
+ * per-tick field-and-cell hot path.
+ *
+ * Plain C: fixed-width integers, plain pointers and sizes, an int32 status on
+ * every call, no exceptions and no torch/CUDA types in any signature (a CUDA
+ * stream travels as `void*`).  Host buffers are caller-allocated.
+ *
+ * Reference interface each group replaces (paths are inside the MARL-OCHRE
+ * workspace):
+ *   - marl_sim_params           crates/marl-config/src/lib.rs:41-106 (SimulationConfig)
+ *   - marl_sim_params_default   crates/marl-config/src/lib.rs:108-168 (Default impl)
+ *   - marl_status               crates/marl-gpu/src/context.rs:5-10 (GpuError)
+ *   - marl_cell / marl_ruleset  crates/marl-cell/src/cell.rs:50-183 (CellState, Ruleset)
+ *   - marl_ctx_create           crates/marl-gpu/src/field_diffusion.rs:32 (GpuFieldDiffuser::new)
+ *   - marl_diffuse_tick_with_cells
+ *                               crates/marl-gpu/src/field_diffusion.rs:158-268
+ *                               (GpuFieldDiffuser::diffuse_tick_with_cells) and
+ *                               crates/marl-field/src/field.rs:212-217
+ *   - marl_apply_boundary_sources  crates/marl-field/src/field.rs:231-250
+ *   - marl_diffuse              crates/marl-field/src/field.rs:107-217
+ *   - marl_light_update         crates/marl-field/src/light.rs:29-59
+ *   - marl_cell_phase           crates/marl-sim/src/lib.rs:206-217 (cell loop:
+ *                               spatial.rs:56-110 gather/scatter + cell.rs:193-369 tick)
+ *   - marl_tick                 crates/marl-sim/src/lib.rs:164-217 (steps 1-4 of a tick)
+ *   - marl_apply_edits          crates/marl-sim/src/lib.rs:220-277 (fate results:
+ *                               halving, swap_remove deaths, appended births)
+ *   - marl_engine_*             crates/marl-sim/src/lib.rs:34-277 (run(): seeding
+ *                               and the tick loop, without file output)
+ *
+ * Threading: one stream per context; a context is not thread-safe, distinct
+ * contexts may be used from distinct host threads.
+ */
+#ifndef MARL_CUDA_H
+#define MARL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Compile-time species/ruleset counts (crates/marl-config/src/lib.rs:22-29).
+ * The grid size is a runtime parameter here (the reference fixes it at
+ * compile time, lib.rs:17-19). */
+#define MARL_S_EXT 12
+#define MARL_M_INT 16
+#define MARL_R_MAX 16
+#define MARL_S_RECEPTORS 8
+#define MARL_S_TRANSPORTERS 8
+#define MARL_S_EFFECTORS 8
+#define MARL_NO_COFACTOR 0xFF
+
+/* Status codes.  GpuError::{NoAdapter, DeviceRequest, BufferMap, InvalidInput}
+ * map to NO_DEVICE, CUDA, CUDA, INVALID_INPUT. */
+typedef enum marl_status {
+    MARL_OK = 0,
+    MARL_ERR_INVALID_INPUT = 1,
+    MARL_ERR_NO_DEVICE = 2,
+    MARL_ERR_CUDA = 3,
+    MARL_ERR_OUT_OF_MEMORY = 4,
+    MARL_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+    MARL_ERR_CAPACITY = 6,  /* cell table or change list capacity exceeded */
+    MARL_ERR_STATE = 7      /* call not valid in the context's current state */
+} marl_status;
+
+/* Cell events returned by the tick (crates/marl-cell/src/cell.rs:155-160). */
+enum {
+    MARL_EVENT_NONE = 0,
+    MARL_EVENT_DIVISION = 1,
+    MARL_EVENT_DEATH = 2,
+    MARL_EVENT_QUIESCENCE = 3
+};
+
+/* Boundary source modes.  ADDITIVE is the reference (field.rs:231-250:
+ * c = min(c + rate, c_max)).  DIRICHLET is a microbenchmark option that pins
+ * the sourced planes to the boundary_prime_* values. */
+enum {
+    MARL_SOURCES_ADDITIVE = 0,
+    MARL_SOURCES_DIRICHLET = 1
+};
+
+/* SimulationConfig, field for field and in declaration order
+ * (crates/marl-config/src/lib.rs:41-106).  usize/u16/u8 fields are widened
+ * to uint32_t.  `source_mode` is an extension (see above). */
+typedef struct marl_sim_params {
+    float dx;
+    float dt;
+    uint32_t diffusion_substeps;
+    float d_voxel[MARL_S_EXT];
+    float lambda_decay[MARL_S_EXT];
+    float source_rate_oxidant;
+    float source_rate_carbon;
+    float source_rate_reductant;
+    float epsilon;
+    float c_max;
+    float lambda_maintenance;
+    float hard_death_floor;
+    float reaction_maintenance;
+    float base_division_prep;
+    float prep_maintenance_multiplier;
+    float rush_penalty_rate;
+    float alpha_eps;
+    float k_eps;
+    float light_efficiency;
+    float surface_intensity;
+    float cell_absorption;
+    float chemical_absorption;
+    float light_floor;
+    float mutation_stddev;
+    float structural_mutation_rate_mult;
+    float meta_mutation_rate;
+    float meta_mutation_clamp_low;
+    float meta_mutation_clamp_high;
+    float hill_exponent_clamp_low;
+    float hill_exponent_clamp_high;
+    float active_reaction_threshold;
+    uint32_t seed_margin;
+    float phototroph_z_lo;
+    float phototroph_z_hi;
+    float chemolithotroph_z_lo;
+    float chemolithotroph_z_hi;
+    float anaerobe_z_lo;
+    float anaerobe_z_hi;
+    uint32_t division_neighbor_distance;
+    uint32_t boundary_prime_layers;
+    float boundary_prime_oxidant;
+    float boundary_prime_carbon;
+    float boundary_prime_reductant;
+    uint32_t source_mode;
+} marl_sim_params;
+
+/* Ruleset pieces (crates/marl-cell/src/cell.rs:50-151), naturally aligned.
+ * The canonical packed 536-byte on-disk form (crates/marl-format/src/lib.rs:70-89)
+ * is produced by marl_ruleset_pack_canonical. */
+typedef struct marl_receptor_params {
+    float k_half, n_hill, gain;
+} marl_receptor_params;
+
+typedef struct marl_transport_params {
+    float uptake_rate, secrete_rate;
+    uint8_t ext_species, int_species, _pad[2];
+} marl_transport_params;
+
+typedef struct marl_reaction {
+    uint8_t substrate, product, catalyst, cofactor;
+    float k_m, v_max, k_cat;
+} marl_reaction;
+
+typedef struct marl_effector_params {
+    float threshold, rate;
+    uint8_t int_species, ext_species, _pad[2];
+} marl_effector_params;
+
+typedef struct marl_fate_params {
+    float division_energy, death_energy, quiescence_energy, division_prep_ticks;
+} marl_fate_params;
+
+typedef struct marl_ruleset {
+    marl_receptor_params receptors[MARL_S_RECEPTORS];
+    marl_transport_params transport[MARL_S_TRANSPORTERS];
+    marl_reaction reactions[MARL_R_MAX];
+    marl_effector_params effectors[MARL_S_EFFECTORS];
+    marl_fate_params fate;
+    float hgt_propensity;
+    float mutation_rate;
+} marl_ruleset; /* 568 bytes */
+
+/* CellState (crates/marl-cell/src/cell.rs:169-183). 656 bytes. */
+typedef struct marl_cell {
+    uint16_t pos[3];
+    uint8_t quiescent;
+    uint8_t starter_type;
+    uint32_t age;
+    uint16_t prep_remaining;
+    uint16_t _pad0;
+    uint64_t lineage_id;
+    float internal[MARL_M_INT];
+    marl_ruleset ruleset;
+} marl_cell;
+
+/* One entry of the compacted per-tick change list: a Division or Death event
+ * of cell `cell` (its index in the cell vector at the start of the tick), in
+ * ascending cell order.  For divisions `internal`/`quiescent` hold the
+ * parent's post-tick state, which the host clones into the daughter
+ * (crates/marl-sim/src/lib.rs:223-245). 72 bytes. */
+typedef struct marl_change {
+    uint32_t cell;
+    uint8_t event;
+    uint8_t quiescent;
+    uint16_t _pad;
+    float internal[MARL_M_INT];
+} marl_change;
+
+/* Result of the host fate step (crates/marl-sim/src/lib.rs:220-277), applied
+ * to the device cell table in this order:
+ *   1. halve[]      parents whose 16 internal species are multiplied by 0.5
+ *                   (indices at the start of the tick)
+ *   2. deaths[]     ascending, unique; their voxels become empty
+ *   3. moves        swap_remove result: slot move_dst[k] (< n_after_deaths)
+ *                   receives the cell from slot move_src[k] (>= n_after_deaths)
+ *   4. births[]     appended at n_after_deaths, n_after_deaths+1, ...
+ */
+typedef struct marl_edit_list {
+    uint32_t n_halve;
+    const uint32_t* halve;
+    uint32_t n_deaths;
+    const uint32_t* deaths;
+    uint32_t n_moves;
+    const uint32_t* move_dst;
+    const uint32_t* move_src;
+    uint32_t n_after_deaths;
+    uint32_t n_births;
+    const marl_cell* births;
+} marl_edit_list;
+
+typedef struct marl_ctx marl_ctx;
+
+/* ---- parameters, errors ------------------------------------------------ */
+marl_status marl_sim_params_default(marl_sim_params* out);
+/* Message of the last failed call on this host thread ("" if none). */
+const char* marl_last_error(void);
+/* Library/ABI version: 0xMMmmpp. */
+uint32_t marl_abi_version(void);
+
+/* ---- context (device-resident field, light, occupancy, cell table) ------ */
+marl_status marl_ctx_create(int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
+                            uint32_t cell_capacity, marl_ctx** out);
+void marl_ctx_destroy(marl_ctx* ctx);
+marl_status marl_ctx_set_stream(marl_ctx* ctx, void* cuda_stream);
+marl_status marl_ctx_set_params(marl_ctx* ctx, const marl_sim_params* sim);
+/* Waits for the context's stream and reports device-side errors. */
+marl_status marl_ctx_synchronize(marl_ctx* ctx);
+/* Diffusion tile shape (index into the kernel's tile table) and z-chunk.
+ * Every choice gives bit-identical results; only speed differs. */
+marl_status marl_ctx_set_tile(marl_ctx* ctx, int32_t tile, int32_t zc);
+marl_status marl_ctx_get_tile(marl_ctx* ctx, int32_t* tile, int32_t* zc);
+/* Tile autotuner (no reference counterpart): times `reps` substeps of every
+ * tile shape / z-chunk candidate on this context's grid with CUDA events and
+ * keeps the fastest.  The live field is not modified. */
+marl_status marl_ctx_autotune(marl_ctx* ctx, int32_t reps, float* best_us_per_substep);
+
+/* Cumulative counters of a context (no reference counterpart; used for
+ * measurement).  device_us sums the CUDA-event spans, on the context's
+ * stream, of the device work of every marl_tick (kernels and the change-list
+ * copy) and marl_apply_edits (edit copy and kernels).  Synchronizes first. */
+typedef struct marl_counters {
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
+    uint64_t kernel_launches;
+    uint64_t ticks;
+    double device_us;
+} marl_counters;
+marl_status marl_ctx_counters(marl_ctx* ctx, marl_counters* out);
+
+marl_status marl_upload_field(marl_ctx* ctx, const float* field /* [z][y][x][12] */);
+marl_status marl_download_field(marl_ctx* ctx, float* field);
+marl_status marl_upload_light(marl_ctx* ctx, const float* light /* [z][y][x] */);
+marl_status marl_download_light(marl_ctx* ctx, float* light);
+/* Replaces the cell table; occupancy follows the cells' positions. Duplicate
+ * or out-of-grid positions are rejected. */
+marl_status marl_upload_cells(marl_ctx* ctx, const marl_cell* cells, uint32_t n);
+marl_status marl_download_cells(marl_ctx* ctx, marl_cell* out, uint32_t cap, uint32_t* n_out);
+marl_status marl_cell_count(marl_ctx* ctx, uint32_t* n_out);
+marl_status marl_download_occupancy(marl_ctx* ctx, uint8_t* occ /* [z][y][x] 0/1 */);
+
+/* ---- per-phase entry points --------------------------------------------- */
+marl_status marl_apply_boundary_sources(marl_ctx* ctx);
+/* `substeps` diffusion substeps with dt_sub = dt / sim.diffusion_substeps.
+ * With fuse_sources != 0 the boundary sources are applied inside the first
+ * substep (same result as marl_apply_boundary_sources followed by
+ * marl_diffuse with fuse_sources = 0). */
+marl_status marl_diffuse(marl_ctx* ctx, uint32_t substeps, int32_t fuse_sources);
+marl_status marl_light_update(marl_ctx* ctx);
+/* The sequential cell loop of one tick on the current field and light.
+ * events_out (nullable) receives one MARL_EVENT_* per cell. */
+marl_status marl_cell_phase(marl_ctx* ctx, uint8_t* events_out);
+/* Steps 1-4 of a tick (sources, diffusion, light, cell loop) and the
+ * compacted change list of Division/Death events copied to `changes`.
+ * *n_changes gets the total count; MARL_ERR_CAPACITY if it exceeds cap (the
+ * first cap entries are still written). */
+marl_status marl_tick(marl_ctx* ctx, marl_change* changes, uint32_t cap, uint32_t* n_changes);
+marl_status marl_apply_edits(marl_ctx* ctx, const marl_edit_list* edits);
+/* Per-species sum of the field in FP64, fixed reduction order. */
+marl_status marl_mass_f64(marl_ctx* ctx, double out[MARL_S_EXT]);
+
+/* GpuFieldDiffuser::diffuse_tick_with_cells: uploads `field` and `occupancy`
+ * (one byte per voxel, nonzero = occupied), runs sim.diffusion_substeps
+ * substeps, and downloads the result into `field`.  substeps == 0 returns
+ * MARL_OK with no work, as the reference does. */
+marl_status marl_diffuse_tick_with_cells(marl_ctx* ctx, float* field, const uint8_t* occupancy);
+
+/* Device-pointer form of the diffusion tick, for callers that own their
+ * device memory.  field_dev holds the input and receives the output;
+ * scratch_dev is a second buffer of the same size (the reference's
+ * Field::scratch, crates/marl-field/src/field.rs:18-20); occupancy_dev is
+ * one byte per voxel.  Stream-ordered on `cuda_stream` (NULL = legacy default
+ * stream); no host synchronisation. */
+marl_status marl_diffuse_device(float* field_dev, float* scratch_dev, const uint8_t* occupancy_dev,
+                                int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
+                                uint32_t substeps, void* cuda_stream);
+
+/* ---- formats ------------------------------------------------------------ */
+/* Canonical 536-byte ruleset payload (crates/marl-format/src/lib.rs:70-89). */
+marl_status marl_ruleset_pack_canonical(const marl_ruleset* rs, uint8_t out[536]);
+marl_status marl_ruleset_unpack_canonical(const uint8_t in[536], marl_ruleset* rs);
+
+/* ---- engine: the tick loop of marl_sim::run over a context -------------- */
+typedef struct marl_engine marl_engine;
+
+typedef struct marl_engine_stats {
+    uint64_t tick;
+    uint64_t population;
+    uint64_t total_divisions;
+    uint64_t total_deaths;
+    uint64_t tick_divisions;
+    uint64_t tick_deaths;
+    uint64_t h2d_bytes_last_tick;
+    uint64_t d2h_bytes_last_tick;
+} marl_engine_stats;
+
+/* init_field_boundaries + seed_cells x3 (crates/marl-sim/src/seeding.rs:9-58,
+ * lib.rs:59-105) with a seeded host RNG (xoshiro256** seeded by splitmix64). */
+marl_status marl_engine_create(int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
+                               uint64_t rng_seed, uint32_t seed_count, uint32_t cell_capacity,
+                               marl_engine** out);
+/* Engine over a caller-provided state (field + cells). */
+marl_status marl_engine_create_from_state(int32_t gx, int32_t gy, int32_t gz,
+                                          const marl_sim_params* sim, uint64_t rng_seed,
+                                          const float* field, const marl_cell* cells, uint32_t n,
+                                          uint32_t cell_capacity, marl_engine** out);
+void marl_engine_destroy(marl_engine* e);
+marl_status marl_engine_set_stream(marl_engine* e, void* cuda_stream);
+/* `ticks` iterations of lib.rs:160-277: device tick, change list to host,
+ * fate processing with the host RNG, edit list to device. */
+marl_status marl_engine_step(marl_engine* e, uint32_t ticks);
+marl_status marl_engine_stats_get(marl_engine* e, marl_engine_stats* out);
+/* Full cell vector in the reference's Vec order. */
+marl_status marl_engine_get_cells(marl_engine* e, marl_cell* out, uint32_t cap, uint32_t* n_out);
+marl_status marl_engine_get_field(marl_engine* e, float* field);
+marl_status marl_engine_get_light(marl_engine* e, float* light);
+marl_ctx* marl_engine_ctx(marl_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MARL_CUDA_H */

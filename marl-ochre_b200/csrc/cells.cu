@@ -1,0 +1,632 @@
+// Cell kernels: neighbour schedule, the cell update (gather -> tick -> scatter)
+// in the reference's sequential order, ordered event compaction, and cell-table
+// edits (halving, deaths, swap_remove moves, births).
+//
+// The reference updates cells one after another in Vec order and applies each
+// cell's field deltas immediately (crates/marl-sim/src/lib.rs:206-217), so cell
+// j reads the field as cells 0..j-1 left it.  Cell j reads and writes exactly
+// the empty face-neighbour voxels N(j) (crates/marl-sim/src/spatial.rs:18-110);
+// occupancy does not change during the loop.  Two cells therefore interact
+// only through a shared empty voxel, and for every empty voxel v the cells
+// touching it form a chain in index order.  The schedule kernel records, for
+// every face f of cell j whose voxel v is empty, dep[f][j] = the largest cell
+// index i < j that also touches v.  The update kernel hands out cells in
+// ascending index order (warp tickets from an atomic counter) and a cell
+// starts only after its <= 6 dependencies have published their `done` epoch.
+// This reproduces the sequential result bit-for-bit while independent cells
+// run in parallel.  Progress: a cell only waits for smaller indices, which
+// were ticketed earlier by warps that are already resident; every wait is
+// bounded and reports kErrTimeoutDeps on expiry.
+//
+// This file is compiled with -fmad=false; every expression keeps the
+// reference's operation order (crates/marl-cell/src/cell.rs:193-369).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace marl {
+
+__constant__ int c_face[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+// ---------------------------------------------------------- schedule -----
+__global__ void k_cell_schedule(CellTable t, uint32_t n, Grid g, const int32_t* __restrict__ cmap) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t P = t.pos[j];
+    const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
+    uint32_t nb = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int nx = x + c_face[f][0], ny = y + c_face[f][1], nz = z + c_face[f][2];
+        int dep = -1;
+        if (nx >= 0 && nx < g.X && ny >= 0 && ny < g.Y && nz >= 0 && nz < g.Z &&
+            cmap[((size_t)nz * g.Y + ny) * g.X + nx] < 0) {
+            nb |= 1u << f;
+#pragma unroll
+            for (int h = 0; h < 6; ++h) {
+                const int ux = nx + c_face[h][0], uy = ny + c_face[h][1], uz = nz + c_face[h][2];
+                if (ux >= 0 && ux < g.X && uy >= 0 && uy < g.Y && uz >= 0 && uz < g.Z) {
+                    const int32_t i = cmap[((size_t)uz * g.Y + uy) * g.X + ux];
+                    if (i >= 0 && (uint32_t)i < j && i > dep) dep = i;
+                }
+            }
+        }
+        t.dep[(size_t)f * t.cap + j] = dep;
+    }
+    t.nb[j] = nb;
+}
+
+// ------------------------------------------------------------ update -----
+constexpr int kTickThreads = 128;
+
+struct CellScratch {  // per-thread arrays indexed dynamically: [k][thread]
+    float x[MARL_M_INT][kTickThreads];
+    float ext[MARL_S_EXT][kTickThreads];
+    float del[MARL_S_EXT][kTickThreads];
+};
+
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void st4(float* p, float4 v) { __stcg(reinterpret_cast<float4*>(p), v); }
+
+__device__ __forceinline__ float rclamp(float v, float lo, float hi) {  // Rust f32::clamp (keeps NaN)
+    if (v < lo) v = lo;
+    if (v > hi) v = hi;
+    return v;
+}
+
+__device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uint32_t nb) {
+    const int tid = threadIdx.x;
+    const CellTable& t = a.t;
+    const size_t cap = t.cap;
+    const Grid g = a.g;
+    const uint32_t P = t.pos[j];
+    const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
+    const size_t vox = ((size_t)z * g.Y + y) * g.X + x;
+    const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
+                              -(long long)g.X * g.Y};
+    const int n = __popc(nb);
+
+    // Gather: mean of the empty face neighbours (spatial.rs:56-77).
+#pragma unroll
+    for (int s = 0; s < 12; ++s) S.ext[s][tid] = 0.0f;
+    for (int f = 0; f < 6; ++f) {
+        if (!((nb >> f) & 1u)) continue;
+        const float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
+        const float4 q0 = ld4(v), q1 = ld4(v + 4), q2 = ld4(v + 8);
+        const float vals[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
+#pragma unroll
+        for (int s = 0; s < 12; ++s) S.ext[s][tid] = S.ext[s][tid] + vals[s];
+    }
+    if (n > 0) {
+        const float nf = (float)n;
+#pragma unroll
+        for (int s = 0; s < 12; ++s) S.ext[s][tid] = S.ext[s][tid] / nf;
+    }
+
+    // CellState::tick (cell.rs:193-369).  Phase 1 (receptors) only writes an
+    // unused local and is omitted.
+#pragma unroll
+    for (int k = 0; k < MARL_M_INT; ++k) S.x[k][tid] = t.internal[k * cap + j];
+#pragma unroll
+    for (int s = 0; s < 12; ++s) S.del[s][tid] = 0.0f;
+    const CellConsts& c = a.k;
+    const float dt = c.dt;
+
+    // Phase 2: transport (cell.rs:223-238)
+    const uint4 tpi = t.tp_idx[j];
+    const uint32_t tpw[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
+#pragma unroll
+    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
+        const uint32_t pair = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+        const uint32_t e = pair & 0xFF, k = pair >> 8;
+        if (e >= MARL_S_EXT || k >= MARL_M_INT) continue;
+        const float2 r = t.tp_rate[i * cap + j];
+        const float ev = S.ext[e][tid];
+        const float xk = S.x[k][tid];
+        const float uptake = r.x * ev / (1.0f + ev);
+        const float secretion = r.y * xk / (1.0f + xk);
+        S.x[k][tid] = rclamp(xk + (uptake - secretion) * dt, 0.0f, c.c_max);
+        S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
+    }
+    S.x[MARL_M_INT - 1][tid] = a.light[vox];  // cell.rs:243
+
+    // Phase 3: reactions, strictly in slot order (cell.rs:246-285)
+    const float feps = 1.1920928955078125e-07f;
+    int active = 0;
+#pragma unroll 4
+    for (int r = 0; r < MARL_R_MAX; ++r) {
+        const uint4 q = t.rx[r * cap + j];
+        const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF, ci = (q.x >> 16) & 0xFF, fi = q.x >> 24;
+        const float km = __uint_as_float(q.y), vmax = __uint_as_float(q.z), kcat = __uint_as_float(q.w);
+        if (fabsf(vmax) > c.thr && si != pi) ++active;
+        if (fabsf(vmax) < c.thr) continue;
+        if (si == pi) continue;
+        if (si >= MARL_M_INT || pi >= MARL_M_INT || ci >= MARL_M_INT) continue;
+        const float s = S.x[si][tid];
+        const float cc = S.x[ci][tid];
+        const float substrate_term = s / (km + s + feps);
+        const float catalyst_term = c.epsilon + cc / (kcat + cc + feps);
+        float rate = vmax * substrate_term * catalyst_term;
+        if (fi != MARL_NO_COFACTOR && fi < MARL_M_INT) {
+            const float cof = S.x[fi][tid];
+            rate *= cof / (1.0f + cof);
+            const float consumed = fminf(0.5f * rate * dt, S.x[fi][tid]);
+            S.x[fi][tid] = S.x[fi][tid] - consumed;
+        }
+        const float flux = fminf(rate * dt, S.x[si][tid]);
+        S.x[si][tid] = S.x[si][tid] - flux;
+        S.x[pi][tid] = fminf(S.x[pi][tid] + flux, c.c_max);
+    }
+
+    // Maintenance (cell.rs:291-311)
+    uint32_t st = t.state[j];
+    uint32_t prep = st & 0xFFFFu;
+    uint32_t quiescent = (st >> 16) & 1u;
+    const float4 fate = t.fate[j];
+    float pm;
+    if (prep > 0) {
+        const float evolved = fmaxf(fate.w, 1.0f);
+        const float rush = fmaxf(c.base_division_prep - evolved, 0.0f);
+        pm = c.prep_maintenance_multiplier + rush * c.rush_penalty_rate;
+    } else {
+        pm = 1.0f;
+    }
+    float x0 = S.x[0][tid];
+    x0 *= 1.0f - c.lambda_maintenance * pm * dt;
+    x0 = fmaxf(x0 - (float)active * c.reaction_maintenance * dt, 0.0f);
+    S.x[0][tid] = x0;
+
+    // Phase 4: effectors (cell.rs:314-329)
+    if (!quiescent) {
+        const uint4 efi = t.ef_idx[j];
+        const uint32_t efw[4] = {efi.x, efi.y, efi.z, efi.w};
+#pragma unroll
+        for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
+            const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+            const uint32_t k = pair & 0xFF, e = pair >> 8;
+            if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
+            const float2 pr = t.ef_par[i * cap + j];
+            const float xk = S.x[k][tid];
+            if (xk > pr.x) {
+                const float amount = pr.y * xk / (1.0f + xk) * dt;
+                S.x[k][tid] = fmaxf(xk - amount, 0.0f);
+                S.del[e][tid] = S.del[e][tid] + amount;
+            }
+        }
+    }
+
+    // Phase 5: fate (cell.rs:332-366)
+    const float energy = S.x[0][tid];
+    t.age[j] = t.age[j] + 1;
+    const float eff_death = fmaxf(fate.y, c.hard_death_floor);
+    uint8_t event;
+    if (energy < eff_death) {
+        prep = 0;
+        event = MARL_EVENT_DEATH;
+    } else if (prep > 0) {
+        prep -= 1;
+        event = prep == 0 ? MARL_EVENT_DIVISION : MARL_EVENT_NONE;
+    } else if (energy > fate.x) {
+        const float pt = fmaxf(fate.w, 1.0f);  // `as u16` saturates
+        prep = pt >= 65535.0f ? 65535u : (uint32_t)pt;
+        quiescent = 0;
+        event = MARL_EVENT_NONE;
+    } else if (energy < fate.z) {
+        quiescent = 1;
+        event = MARL_EVENT_QUIESCENCE;
+    } else {
+        quiescent = 0;
+        event = MARL_EVENT_NONE;
+    }
+    t.state[j] = (st & 0xFF000000u) | (quiescent << 16) | prep;
+    t.events[j] = event;
+#pragma unroll
+    for (int k = 0; k < MARL_M_INT; ++k) t.internal[k * cap + j] = S.x[k][tid];
+
+    // Scatter: split deltas over the same neighbours, clamp after each add
+    // (spatial.rs:87-110, field.rs:57-62).
+    if (n > 0) {
+        const float nf = (float)n;
+        float split[12];
+#pragma unroll
+        for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] / nf;
+        for (int f = 0; f < 6; ++f) {
+            if (!((nb >> f) & 1u)) continue;
+            float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
+            float4 q0 = ld4(v), q1 = ld4(v + 4), q2 = ld4(v + 8);
+            q0 = make_float4(fmaxf(q0.x + split[0], 0.0f), fmaxf(q0.y + split[1], 0.0f), fmaxf(q0.z + split[2], 0.0f),
+                             fmaxf(q0.w + split[3], 0.0f));
+            q1 = make_float4(fmaxf(q1.x + split[4], 0.0f), fmaxf(q1.y + split[5], 0.0f), fmaxf(q1.z + split[6], 0.0f),
+                             fmaxf(q1.w + split[7], 0.0f));
+            q2 = make_float4(fmaxf(q2.x + split[8], 0.0f), fmaxf(q2.y + split[9], 0.0f),
+                             fmaxf(q2.z + split[10], 0.0f), fmaxf(q2.w + split[11], 0.0f));
+            st4(v, q0);
+            st4(v + 4, q1);
+            st4(v + 8, q2);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick(CellLaunch a) {
+    __shared__ CellScratch S;
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const CellTable& t = a.t;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(a.ticket, 32u);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= a.n) break;
+        const uint32_t j = base + lane;
+        bool pending = j < a.n;
+        const uint32_t nb = pending ? t.nb[j] : 0u;
+        uint32_t spins = 0;
+        while (__any_sync(FULL, pending)) {
+            if (pending) {
+                bool ready = true;
+                for (int f = 0; f < 6; ++f) {
+                    if (!((nb >> f) & 1u)) continue;
+                    const int32_t d = t.dep[(size_t)f * t.cap + j];
+                    if (d >= 0 && ld_acquire_u32(&t.done[d]) != a.epoch) ready = false;
+                }
+                if (ready) {
+                    update_cell(a, S, j, nb);
+                    __threadfence();
+                    st_release_u32(&t.done[j], a.epoch);
+                    pending = false;
+                }
+            }
+            if (__any_sync(FULL, pending)) {
+                if (++spins > kFlagSpinLimit) {
+                    if (pending) {
+                        atomicOr(a.err, kErrTimeoutDeps);
+                        t.events[j] = MARL_EVENT_NONE;
+                        st_release_u32(&t.done[j], a.epoch);
+                        pending = false;
+                    }
+                } else {
+                    __nanosleep(64);
+                }
+            }
+        }
+    }
+}
+
+// -------------------------------------------------------- compaction -----
+constexpr int kCompactThreads = 256;
+constexpr int kCompactPerThread = 4;
+constexpr int kCompactPerBlock = kCompactThreads * kCompactPerThread;
+
+__device__ __forceinline__ bool is_change(uint8_t e) { return e == MARL_EVENT_DIVISION || e == MARL_EVENT_DEATH; }
+
+__global__ void __launch_bounds__(kCompactThreads) k_count_events(const uint8_t* __restrict__ ev, uint32_t n,
+                                                                  uint32_t* __restrict__ block_counts) {
+    __shared__ uint32_t warp_sums[kCompactThreads / 32];
+    const uint32_t first = blockIdx.x * kCompactPerBlock + threadIdx.x * kCompactPerThread;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int i = 0; i < kCompactPerThread; ++i) cnt += (first + i < n && is_change(ev[first + i])) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (int w = 0; w < kCompactThreads / 32; ++w) s += warp_sums[w];
+        block_counts[blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_scatter_events(CellTable t, uint32_t n,
+                                                                    const uint32_t* __restrict__ block_counts,
+                                                                    ChangeHeader* hdr, marl_change* __restrict__ out,
+                                                                    uint32_t cap) {
+    __shared__ uint32_t red[kCompactThreads];
+    __shared__ uint32_t warp_tot[kCompactThreads / 32];
+    // offset of this block = sum of the counts of earlier blocks
+    uint32_t part = 0;
+    for (uint32_t b = threadIdx.x; b < blockIdx.x; b += kCompactThreads) part += block_counts[b];
+    red[threadIdx.x] = part;
+    __syncthreads();
+    for (int w = kCompactThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const uint32_t block_off = red[0];
+    const uint32_t first = blockIdx.x * kCompactPerBlock + threadIdx.x * kCompactPerThread;
+    uint32_t flags = 0, cnt = 0;
+#pragma unroll
+    for (int i = 0; i < kCompactPerThread; ++i)
+        if (first + i < n && is_change(t.events[first + i])) {
+            flags |= 1u << i;
+            ++cnt;
+        }
+    // exclusive scan of cnt over the block, in thread (= cell) order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    uint32_t warp_off = 0;
+    for (int w = 0; w < warp; ++w) warp_off += warp_tot[w];
+    uint32_t pos = block_off + warp_off + incl - cnt;
+    for (int i = 0; i < kCompactPerThread; ++i) {
+        if (!((flags >> i) & 1u)) continue;
+        const uint32_t j = first + i;
+        if (pos < cap) {
+            marl_change& r = out[pos];
+            r.cell = j;
+            r.event = t.events[j];
+            r.quiescent = (uint8_t)((t.state[j] >> 16) & 1u);
+            r._pad = 0;
+            for (int k = 0; k < MARL_M_INT; ++k) r.internal[k] = t.internal[(size_t)k * t.cap + j];
+        }
+        ++pos;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kCompactThreads - 1) {
+        hdr->count = pos;
+        hdr->n_cells = n;
+    }
+}
+
+// ------------------------------------------------------------- edits -----
+__device__ void write_record(CellTable& t, uint32_t slot, const marl_cell& c) {
+    const size_t cap = t.cap;
+    t.pos[slot] = pack_pos(c.pos[0], c.pos[1], c.pos[2]);
+    t.age[slot] = c.age;
+    t.state[slot] = (uint32_t)c.prep_remaining | ((uint32_t)(c.quiescent ? 1 : 0) << 16) |
+                    ((uint32_t)c.starter_type << 24);
+    t.lineage[slot] = c.lineage_id;
+    for (int k = 0; k < MARL_M_INT; ++k) t.internal[k * cap + slot] = c.internal[k];
+    const marl_ruleset& r = c.ruleset;
+    uint32_t w[4] = {0, 0, 0, 0};
+    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
+        t.tp_rate[i * cap + slot] = make_float2(r.transport[i].uptake_rate, r.transport[i].secrete_rate);
+        w[i >> 1] |= ((uint32_t)r.transport[i].ext_species | ((uint32_t)r.transport[i].int_species << 8))
+                     << ((i & 1) * 16);
+    }
+    t.tp_idx[slot] = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int i = 0; i < MARL_R_MAX; ++i) {
+        const marl_reaction& q = r.reactions[i];
+        const uint32_t idx = (uint32_t)q.substrate | ((uint32_t)q.product << 8) | ((uint32_t)q.catalyst << 16) |
+                             ((uint32_t)q.cofactor << 24);
+        t.rx[i * cap + slot] = make_uint4(idx, __float_as_uint(q.k_m), __float_as_uint(q.v_max), __float_as_uint(q.k_cat));
+    }
+    uint32_t e[4] = {0, 0, 0, 0};
+    for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
+        t.ef_par[i * cap + slot] = make_float2(r.effectors[i].threshold, r.effectors[i].rate);
+        e[i >> 1] |= ((uint32_t)r.effectors[i].int_species | ((uint32_t)r.effectors[i].ext_species << 8))
+                     << ((i & 1) * 16);
+    }
+    t.ef_idx[slot] = make_uint4(e[0], e[1], e[2], e[3]);
+    t.fate[slot] = make_float4(r.fate.division_energy, r.fate.death_energy, r.fate.quiescence_energy,
+                               r.fate.division_prep_ticks);
+    float* cold = t.cold + (size_t)slot * kColdFloats;
+    for (int i = 0; i < MARL_S_RECEPTORS; ++i) {
+        cold[3 * i] = r.receptors[i].k_half;
+        cold[3 * i + 1] = r.receptors[i].n_hill;
+        cold[3 * i + 2] = r.receptors[i].gain;
+    }
+    cold[24] = r.hgt_propensity;
+    cold[25] = r.mutation_rate;
+}
+
+__global__ void k_cells_from_records(const marl_cell* __restrict__ rec, uint32_t count, uint32_t base, CellTable t,
+                                     Grid g, int32_t* __restrict__ cmap, uint8_t* __restrict__ mask,
+                                     uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const marl_cell& c = rec[i];
+    if (c.pos[0] >= g.X || c.pos[1] >= g.Y || c.pos[2] >= g.Z) {
+        atomicOr(err, kErrBadIndex);
+        return;
+    }
+    const uint32_t slot = base + i;
+    write_record(t, slot, c);
+    const size_t row = (size_t)c.pos[2] * g.Y + c.pos[1];
+    cmap[row * g.X + c.pos[0]] = (int32_t)slot;
+    mask[row * mask_pitch(g.X) + c.pos[0]] = 1;
+}
+
+__global__ void k_cells_to_records(CellTable t, uint32_t n, marl_cell* __restrict__ rec) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const size_t cap = t.cap;
+    marl_cell& c = rec[j];
+    const uint32_t P = t.pos[j];
+    c.pos[0] = (uint16_t)pos_x(P);
+    c.pos[1] = (uint16_t)pos_y(P);
+    c.pos[2] = (uint16_t)pos_z(P);
+    const uint32_t st = t.state[j];
+    c.quiescent = (uint8_t)((st >> 16) & 1u);
+    c.starter_type = (uint8_t)(st >> 24);
+    c.age = t.age[j];
+    c.prep_remaining = (uint16_t)(st & 0xFFFFu);
+    c._pad0 = 0;
+    c.lineage_id = t.lineage[j];
+    for (int k = 0; k < MARL_M_INT; ++k) c.internal[k] = t.internal[k * cap + j];
+    marl_ruleset& r = c.ruleset;
+    const uint4 tpi = t.tp_idx[j];
+    const uint32_t w[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
+    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
+        const float2 rr = t.tp_rate[i * cap + j];
+        const uint32_t pair = (w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+        r.transport[i].uptake_rate = rr.x;
+        r.transport[i].secrete_rate = rr.y;
+        r.transport[i].ext_species = (uint8_t)(pair & 0xFF);
+        r.transport[i].int_species = (uint8_t)(pair >> 8);
+        r.transport[i]._pad[0] = r.transport[i]._pad[1] = 0;
+    }
+    for (int i = 0; i < MARL_R_MAX; ++i) {
+        const uint4 q = t.rx[i * cap + j];
+        r.reactions[i].substrate = (uint8_t)(q.x & 0xFF);
+        r.reactions[i].product = (uint8_t)((q.x >> 8) & 0xFF);
+        r.reactions[i].catalyst = (uint8_t)((q.x >> 16) & 0xFF);
+        r.reactions[i].cofactor = (uint8_t)(q.x >> 24);
+        r.reactions[i].k_m = __uint_as_float(q.y);
+        r.reactions[i].v_max = __uint_as_float(q.z);
+        r.reactions[i].k_cat = __uint_as_float(q.w);
+    }
+    const uint4 efi = t.ef_idx[j];
+    const uint32_t e[4] = {efi.x, efi.y, efi.z, efi.w};
+    for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
+        const float2 pr = t.ef_par[i * cap + j];
+        const uint32_t pair = (e[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+        r.effectors[i].threshold = pr.x;
+        r.effectors[i].rate = pr.y;
+        r.effectors[i].int_species = (uint8_t)(pair & 0xFF);
+        r.effectors[i].ext_species = (uint8_t)(pair >> 8);
+        r.effectors[i]._pad[0] = r.effectors[i]._pad[1] = 0;
+    }
+    const float4 f = t.fate[j];
+    r.fate.division_energy = f.x;
+    r.fate.death_energy = f.y;
+    r.fate.quiescence_energy = f.z;
+    r.fate.division_prep_ticks = f.w;
+    const float* cold = t.cold + (size_t)j * kColdFloats;
+    for (int i = 0; i < MARL_S_RECEPTORS; ++i) {
+        r.receptors[i].k_half = cold[3 * i];
+        r.receptors[i].n_hill = cold[3 * i + 1];
+        r.receptors[i].gain = cold[3 * i + 2];
+    }
+    r.hgt_propensity = cold[24];
+    r.mutation_rate = cold[25];
+}
+
+// Division halving (crates/marl-sim/src/lib.rs:237-240): parent internals *= 0.5.
+__global__ void k_halve(CellTable t, const uint32_t* __restrict__ idx, uint32_t count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count * MARL_M_INT) return;
+    const uint32_t p = idx[i / MARL_M_INT];
+    const uint32_t k = i % MARL_M_INT;
+    float& v = t.internal[(size_t)k * t.cap + p];
+    v = v * 0.5f;
+}
+
+// Dead cells leave the occupancy (cell_map.remove, lib.rs:261-262).
+__global__ void k_clear_dead(CellTable t, const uint32_t* __restrict__ idx, uint32_t count, Grid g,
+                             int32_t* __restrict__ cmap, uint8_t* __restrict__ mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t P = t.pos[idx[i]];
+    const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
+    cmap[row * g.X + pos_x(P)] = -1;
+    mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
+}
+
+// swap_remove result (lib.rs:258-267): slot dst receives the cell in slot src.
+// Sources are >= the post-death length and destinations below it, so the
+// copies are independent.
+__global__ void k_moves(CellTable t, const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t count,
+                        Grid g, int32_t* __restrict__ cmap) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t d = dst[i], s = src[i];
+    const size_t cap = t.cap;
+    t.pos[d] = t.pos[s];
+    t.age[d] = t.age[s];
+    t.state[d] = t.state[s];
+    t.lineage[d] = t.lineage[s];
+    for (int k = 0; k < MARL_M_INT; ++k) t.internal[k * cap + d] = t.internal[k * cap + s];
+    for (int k = 0; k < MARL_S_TRANSPORTERS; ++k) t.tp_rate[k * cap + d] = t.tp_rate[k * cap + s];
+    t.tp_idx[d] = t.tp_idx[s];
+    for (int k = 0; k < MARL_R_MAX; ++k) t.rx[k * cap + d] = t.rx[k * cap + s];
+    for (int k = 0; k < MARL_S_EFFECTORS; ++k) t.ef_par[k * cap + d] = t.ef_par[k * cap + s];
+    t.ef_idx[d] = t.ef_idx[s];
+    t.fate[d] = t.fate[s];
+    for (int k = 0; k < kColdFloats; ++k) t.cold[(size_t)d * kColdFloats + k] = t.cold[(size_t)s * kColdFloats + k];
+    const uint32_t P = t.pos[s];
+    cmap[((size_t)pos_z(P) * g.Y + pos_y(P)) * g.X + pos_x(P)] = (int32_t)d;
+}
+
+__global__ void k_rebuild_maps(CellTable t, uint32_t n, Grid g, int32_t* __restrict__ cmap,
+                               uint8_t* __restrict__ mask) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t P = t.pos[j];
+    const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
+    cmap[row * g.X + pos_x(P)] = (int32_t)j;
+    mask[row * mask_pitch(g.X) + pos_x(P)] = 1;
+}
+
+// ======================================================== launchers ======
+static inline unsigned blocks_for(size_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    k_cell_schedule<<<blocks_for(a.n, 256), 256, 0, s>>>(a.t, a.n, a.g, a.cmap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick, kTickThreads, 0);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+    }
+    const uint32_t warps_needed = (a.n + 31) / 32;
+    const uint32_t blocks_needed = (warps_needed + (kTickThreads / 32) - 1) / (kTickThreads / 32);
+    // Persistent: never more blocks than can be resident at once, so every
+    // ticket holder is running (the dependency waits rely on it).
+    const uint32_t resident = (uint32_t)per_sm * (uint32_t)num_sms;
+    const uint32_t blocks = blocks_needed < resident ? blocks_needed : resident;
+    k_cell_tick<<<blocks, kTickThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+uint32_t compaction_blocks(uint32_t n) { return n == 0 ? 1 : (n + kCompactPerBlock - 1) / kCompactPerBlock; }
+
+cudaError_t launch_compact_events(const CellTable& t, uint32_t n, uint32_t* block_counts, ChangeHeader* hdr,
+                                  marl_change* changes, uint32_t cap, cudaStream_t s) {
+    const uint32_t nb = compaction_blocks(n);
+    k_count_events<<<nb, kCompactThreads, 0, s>>>(t.events, n, block_counts);
+    k_scatter_events<<<nb, kCompactThreads, 0, s>>>(t, n, block_counts, hdr, changes, cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cells_from_records(const marl_cell* rec, uint32_t count, uint32_t base, CellTable t, const Grid& g,
+                                      int32_t* cmap, uint8_t* mask, uint32_t* err, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_cells_from_records<<<blocks_for(count, 128), 128, 0, s>>>(rec, count, base, t, g, cmap, mask, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cells_to_records(const CellTable& t, uint32_t n, marl_cell* rec, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_cells_to_records<<<blocks_for(n, 128), 128, 0, s>>>(t, n, rec);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halve(const CellTable& t, const uint32_t* idx, uint32_t count, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_halve<<<blocks_for((size_t)count * MARL_M_INT, 256), 256, 0, s>>>(t, idx, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clear_dead(const CellTable& t, const uint32_t* idx, uint32_t count, const Grid& g, int32_t* cmap,
+                              uint8_t* mask, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_clear_dead<<<blocks_for(count, 256), 256, 0, s>>>(t, idx, count, g, cmap, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_moves(CellTable t, const uint32_t* dst, const uint32_t* src, uint32_t count, const Grid& g,
+                         int32_t* cmap, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_moves<<<blocks_for(count, 128), 128, 0, s>>>(t, dst, src, count, g, cmap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rebuild_maps(const CellTable& t, uint32_t n, const Grid& g, int32_t* cmap, uint8_t* mask,
+                                cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_rebuild_maps<<<blocks_for(n, 256), 256, 0, s>>>(t, n, g, cmap, mask);
+    return cudaGetLastError();
+}
+
+}  // namespace marl

@@ -1,0 +1,83 @@
+// Definition of the opaque marl_ctx (device-resident state of one grid) and
+// helpers shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/marl_cuda.h"
+#include "common.cuh"
+#include "internal.h"
+
+namespace marl {
+
+constexpr uint32_t kPrefetchChanges = 256;  // change-list entries fetched with the header
+
+}  // namespace marl
+
+struct marl_ctx {
+    int device = 0;
+    int num_sms = 0;
+    marl::Grid g{0, 0, 0};
+    marl_sim_params sim{};
+    marl::FieldConsts fk{};
+    marl::CellConsts ck{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    float* field[2] = {nullptr, nullptr};  // ping-pong; field[cur] is live
+    int cur = 0;
+    uint8_t* mask = nullptr;   // [z][y][pitch] occupancy of the cell table
+    int32_t* cmap = nullptr;   // [z][y][x] cell index or -1
+    float* light = nullptr;    // [z][y][x]
+    marl::CellTable t{};
+    uint32_t n = 0;
+    uint32_t epoch = 0;
+    bool schedule_dirty = true;
+    marl::DiffusionPlan plan{};
+
+    marl::ChangeHeader* d_hdr = nullptr;  // device header (count, err, ticket)
+    marl::ChangeHeader* h_hdr = nullptr;  // pinned: header followed by kPrefetchChanges entries
+    marl_change* d_changes = nullptr;
+    uint32_t* d_block_counts = nullptr;
+
+    void* d_edit = nullptr;  // edit-list staging
+    void* h_edit = nullptr;
+    size_t edit_bytes = 0;
+    marl_cell* d_records = nullptr;  // AoS cell records staging
+    marl_cell* h_records = nullptr;
+    uint32_t records_cap = 0;
+
+    double* d_mass_partial = nullptr;
+    double* d_mass_out = nullptr;
+    double* h_mass = nullptr;
+    uint8_t* d_events_stage = nullptr;
+
+    // GpuFieldDiffuser seam: occupancy supplied by the caller
+    uint8_t* d_occ_stage = nullptr;  // dense one byte per voxel
+    uint8_t* d_seam_mask = nullptr;
+    marl::DiffusionPlan seam_plan{};
+
+    uint64_t h2d_bytes = 0;  // transfer counters (engine statistics)
+    uint64_t d2h_bytes = 0;
+    uint64_t launches = 0;   // kernels enqueued by this context
+    uint64_t ticks = 0;
+
+    // Device-time spans: event pairs recorded around the device work of
+    // marl_tick / marl_apply_edits, resolved after the stream has synchronized.
+    struct Span {
+        cudaEvent_t a, b;
+    };
+    std::vector<Span> span_pool, spans_pending;
+    double device_us = 0.0;
+
+    marl_change* h_changes_prefix() {
+        return reinterpret_cast<marl_change*>(reinterpret_cast<uint8_t*>(h_hdr) + sizeof(marl::ChangeHeader));
+    }
+};
+
+namespace marl {
+marl_status fail(marl_status st, const char* fmt, ...);
+marl_status cuda_fail(cudaError_t e, const char* where);
+}  // namespace marl

@@ -1,0 +1,491 @@
+// Host engine: the tick loop of marl_sim::run (crates/marl-sim/src/lib.rs:34-277)
+// over a device context.  Each tick the device runs sources, diffusion, light
+// and the cell loop and returns the ordered change list of Division/Death
+// events; the host then performs the reference's fate processing — division
+// placement, cloning, halving, mutation, lineage draws, swap_remove deaths and
+// appended births — with its seeded RNG, and sends the resulting edit list
+// back.  File output (dumps, CSV, images) is not part of this path.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/marl_cuda.h"
+#include "host_rng.h"
+
+namespace marl {
+marl_status fail(marl_status st, const char* fmt, ...);
+}
+using marl::fail;
+using marl::HostRng;
+
+namespace {
+
+// crates/marl-sim/src/spatial.rs:8-15
+const int kFace[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+float rust_clamp(float v, float lo, float hi) {
+    if (v < lo) v = lo;
+    if (v > hi) v = hi;
+    return v;
+}
+
+// ---- starter metabolisms (crates/marl-sim/src/starter_metabolisms.rs) ----
+void set_inactive(marl_ruleset& r) {  // :6-42
+    std::memset(&r, 0, sizeof(r));
+    for (auto& x : r.receptors) x = marl_receptor_params{1.0f, 2.0f, 0.0f};
+    for (auto& x : r.transport) x = marl_transport_params{0.0f, 0.0f, 0, 0, {0, 0}};
+    for (auto& x : r.reactions) x = marl_reaction{0, 0, 0, MARL_NO_COFACTOR, 1.0f, 0.0f, 0.5f};
+    for (auto& x : r.effectors) x = marl_effector_params{10.0f, 0.0f, 0, 0, {0, 0}};
+}
+
+marl_cell starter(int kind, const uint16_t pos[3], uint64_t lineage) {
+    marl_cell c;
+    std::memset(&c, 0, sizeof(c));
+    std::memcpy(c.pos, pos, sizeof(c.pos));
+    c.lineage_id = lineage;
+    c.starter_type = (uint8_t)kind;
+    marl_ruleset& r = c.ruleset;
+    set_inactive(r);
+    r.hgt_propensity = 0.1f;
+    r.mutation_rate = 0.05f;
+    const uint8_t N = MARL_NO_COFACTOR;
+    if (kind == 0) {  // phototroph, :46-187
+        r.receptors[2] = {0.3f, 2.0f, 1.0f};
+        r.receptors[3] = {0.5f, 2.0f, 1.0f};
+        r.transport[0] = {0.6f, 0.0f, 3, 3, {0, 0}};
+        r.transport[1] = {0.0f, 0.6f, 1, 1, {0, 0}};
+        r.transport[2] = {0.0f, 0.3f, 4, 4, {0, 0}};
+        r.transport[3] = {0.1f, 0.0f, 2, 2, {0, 0}};
+        r.reactions[0] = {3, 0, 15, N, 0.2f, 0.8f, 0.1f};
+        r.reactions[1] = {3, 1, 15, N, 0.2f, 0.4f, 0.1f};
+        r.reactions[2] = {3, 4, 0, N, 0.3f, 0.3f, 0.3f};
+        r.reactions[3] = {3, 5, 6, N, 0.3f, 0.15f, 0.1f};
+        r.reactions[4] = {3, 6, 5, N, 0.3f, 0.1f, 0.1f};
+        r.effectors[0] = {0.5f, 0.8f, 1, 1, {0, 0}};
+        r.effectors[1] = {1.0f, 0.2f, 4, 4, {0, 0}};
+        r.fate = {1.2f, 0.05f, 0.15f, 20.0f};
+        c.internal[0] = 0.3f, c.internal[3] = 0.3f, c.internal[5] = 0.05f, c.internal[6] = 0.05f;
+    } else if (kind == 1) {  // chemolithotroph, :191-326
+        r.receptors[1] = {0.3f, 2.0f, 1.0f};
+        r.receptors[2] = {0.3f, 2.0f, 1.0f};
+        r.transport[0] = {0.7f, 0.0f, 1, 1, {0, 0}};
+        r.transport[1] = {0.7f, 0.0f, 2, 2, {0, 0}};
+        r.transport[2] = {0.2f, 0.0f, 3, 3, {0, 0}};
+        r.transport[3] = {0.0f, 0.3f, 4, 4, {0, 0}};
+        r.reactions[0] = {2, 0, 5, 1, 0.15f, 0.7f, 0.1f};
+        r.reactions[1] = {1, 4, 0, N, 0.3f, 0.3f, 0.2f};
+        r.reactions[2] = {7, 0, 5, N, 0.3f, 0.15f, 0.1f};
+        r.reactions[3] = {3, 5, 6, N, 0.3f, 0.15f, 0.1f};
+        r.reactions[4] = {3, 6, 5, N, 0.3f, 0.1f, 0.1f};
+        r.effectors[0] = {0.5f, 0.3f, 4, 4, {0, 0}};
+        r.fate = {1.0f, 0.05f, 0.12f, 20.0f};
+        c.internal[0] = 1.5f, c.internal[1] = 0.5f, c.internal[2] = 0.5f;
+        c.internal[5] = 0.05f, c.internal[6] = 0.05f, c.internal[7] = 5.0f;
+    } else {  // anaerobe, :330-459
+        r.receptors[2] = {0.3f, 2.0f, 1.0f};
+        r.transport[0] = {0.9f, 0.0f, 2, 2, {0, 0}};
+        r.transport[1] = {0.3f, 0.0f, 3, 3, {0, 0}};
+        r.transport[2] = {0.0f, 0.5f, 4, 4, {0, 0}};
+        r.transport[3] = {0.1f, 0.0f, 1, 1, {0, 0}};
+        r.reactions[0] = {2, 0, 5, N, 0.15f, 0.8f, 0.1f};
+        r.reactions[1] = {3, 4, 0, N, 0.2f, 0.3f, 0.2f};
+        r.reactions[2] = {0, 3, 1, N, 0.01f, 2.0f, 0.01f};
+        r.reactions[3] = {3, 5, 6, N, 0.3f, 0.15f, 0.1f};
+        r.reactions[4] = {3, 6, 5, N, 0.3f, 0.1f, 0.1f};
+        r.effectors[0] = {0.5f, 0.5f, 4, 4, {0, 0}};
+        r.fate = {0.8f, 0.05f, 0.1f, 20.0f};
+        c.internal[0] = 0.5f, c.internal[2] = 0.7f, c.internal[5] = 0.05f, c.internal[6] = 0.05f;
+    }
+    return c;
+}
+
+// ---- Ruleset::mutate (crates/marl-cell/src/cell.rs:406-524) ----
+void perturb(float& v, float rate, float sd, HostRng& rng) {
+    if (rng.f32() < rate) {
+        v += rng.normal(sd);
+        v = std::fmax(v, 0.0f);
+    }
+}
+
+void mutate_ruleset(marl_ruleset& rs, HostRng& rng, const marl_sim_params& sim) {
+    const float rate = rs.mutation_rate;
+    const float sd = sim.mutation_stddev;
+    const float structural = rate * sim.structural_mutation_rate_mult;
+    for (auto& r : rs.receptors) {
+        perturb(r.k_half, rate, sd, rng);
+        perturb(r.n_hill, rate, sd, rng);
+        r.n_hill = rust_clamp(r.n_hill, sim.hill_exponent_clamp_low, sim.hill_exponent_clamp_high);
+        perturb(r.gain, rate, sd, rng);
+    }
+    for (auto& t : rs.transport) {
+        perturb(t.uptake_rate, rate, sd, rng);
+        perturb(t.secrete_rate, rate, sd, rng);
+        if (rng.f32() < structural) t.ext_species = (uint8_t)rng.range(0, MARL_S_EXT);
+        if (rng.f32() < structural) t.int_species = (uint8_t)rng.range(0, MARL_M_INT);
+    }
+    // Gene-duplication donors: reactions active before this mutation pass.
+    std::vector<int> donors;
+    for (int i = 0; i < MARL_R_MAX; ++i)
+        if (std::fabs(rs.reactions[i].v_max) > sim.active_reaction_threshold) donors.push_back(i);
+    for (int i = 0; i < MARL_R_MAX; ++i) {
+        marl_reaction& rx = rs.reactions[i];
+        perturb(rx.k_m, rate, sd, rng);
+        perturb(rx.v_max, rate, sd, rng);
+        perturb(rx.k_cat, rate, sd, rng);
+        uint8_t marl_reaction::*slots[3] = {&marl_reaction::substrate, &marl_reaction::product,
+                                            &marl_reaction::catalyst};
+        for (auto slot : slots) {
+            if (rng.f32() < structural) {
+                const uint32_t pick = rng.range(0, (uint32_t)std::max<size_t>(donors.size(), 1));
+                if (pick < donors.size()) {
+                    const int donor = donors[pick];
+                    if (donor != i) rx.*slot = rs.reactions[donor].*slot;
+                } else {
+                    rx.*slot = (uint8_t)rng.range(0, MARL_M_INT);
+                }
+            }
+        }
+    }
+    for (auto& e : rs.effectors) {
+        perturb(e.threshold, rate, sd, rng);
+        perturb(e.rate, rate, sd, rng);
+    }
+    perturb(rs.fate.division_energy, rate, sd, rng);
+    perturb(rs.fate.death_energy, rate, sd, rng);
+    perturb(rs.fate.quiescence_energy, rate, sd, rng);
+    perturb(rs.fate.division_prep_ticks, rate, sd, rng);
+    rs.fate.division_prep_ticks = std::fmax(rs.fate.division_prep_ticks, 1.0f);
+    perturb(rs.hgt_propensity, rate, sd, rng);
+    if (rng.f32() < sim.meta_mutation_rate) {
+        rs.mutation_rate += rng.normal(sd) * sim.meta_mutation_rate;
+        rs.mutation_rate = rust_clamp(rs.mutation_rate, sim.meta_mutation_clamp_low, sim.meta_mutation_clamp_high);
+    }
+}
+
+// Host-side cell record kept for fate processing: what the device does not
+// change during a tick (position, lineage, starter type, ruleset).
+struct HostCell {
+    uint16_t pos[3];
+    uint8_t starter_type;
+    uint64_t lineage_id;
+    marl_ruleset ruleset;
+};
+
+}  // namespace
+
+struct marl_engine {
+    marl_ctx* ctx = nullptr;
+    int X = 0, Y = 0, Z = 0;
+    marl_sim_params sim{};
+    HostRng rng;
+    std::vector<HostCell> cells;  // the reference's `cells: Vec<CellState>` order
+    std::vector<int32_t> cmap;    // the reference's `cell_map` as a dense voxel map
+    std::vector<marl_change> changes;
+    uint64_t tick = 0, total_div = 0, total_death = 0, tick_div = 0, tick_death = 0;
+    uint64_t h2d_last = 0, d2h_last = 0;
+
+    size_t vox(int x, int y, int z) const { return ((size_t)z * Y + y) * X + x; }
+
+    // crates/marl-sim/src/spatial.rs:115-154 (find_empty_neighbor)
+    bool find_empty_neighbor(const uint16_t p[3], uint16_t out[3]) {
+        const int dist = (int)sim.division_neighbor_distance;
+        uint16_t cand[6][3];
+        uint32_t nc = 0;
+        for (const auto& f : kFace) {
+            const int nx = p[0] + f[0] * dist, ny = p[1] + f[1] * dist, nz = p[2] + f[2] * dist;
+            if (nx >= 0 && nx < X && ny >= 0 && ny < Y && nz >= 0 && nz < Z && cmap[vox(nx, ny, nz)] < 0) {
+                cand[nc][0] = (uint16_t)nx, cand[nc][1] = (uint16_t)ny, cand[nc][2] = (uint16_t)nz;
+                ++nc;
+            }
+        }
+        if (nc == 0) {
+            for (const auto& f : kFace) {
+                const int nx = p[0] + f[0], ny = p[1] + f[1], nz = p[2] + f[2];
+                if (nx >= 0 && nx < X && ny >= 0 && ny < Y && nz >= 0 && nz < Z && cmap[vox(nx, ny, nz)] < 0) {
+                    cand[nc][0] = (uint16_t)nx, cand[nc][1] = (uint16_t)ny, cand[nc][2] = (uint16_t)nz;
+                    ++nc;
+                }
+            }
+            if (nc == 0) return false;
+        }
+        const uint32_t i = rng.range(0, nc);
+        std::memcpy(out, cand[i], sizeof(uint16_t) * 3);
+        return true;
+    }
+
+    // crates/marl-sim/src/lib.rs:219-277 (fate processing) -> edit list
+    marl_status process_changes(uint32_t count) {
+        tick_div = tick_death = 0;
+        std::vector<marl_cell> births;
+        std::vector<uint32_t> halve, deaths;
+        for (uint32_t k = 0; k < count; ++k) {
+            const marl_change& ch = changes[k];
+            if (ch.cell >= cells.size()) return fail(MARL_ERR_STATE, "change list names cell %u of %zu", ch.cell,
+                                                     cells.size());
+            if (ch.event == MARL_EVENT_DIVISION) {
+                const HostCell& parent = cells[ch.cell];
+                uint16_t dpos[3];
+                if (find_empty_neighbor(parent.pos, dpos)) {
+                    marl_cell d;
+                    std::memset(&d, 0, sizeof(d));
+                    std::memcpy(d.pos, dpos, sizeof(dpos));
+                    d.quiescent = ch.quiescent;
+                    d.starter_type = parent.starter_type;
+                    d.age = 0;
+                    d.prep_remaining = 0;
+                    d.lineage_id = rng.u64();
+                    for (int i = 0; i < MARL_M_INT; ++i) d.internal[i] = ch.internal[i] * 0.5f;
+                    d.ruleset = parent.ruleset;
+                    halve.push_back(ch.cell);
+                    mutate_ruleset(d.ruleset, rng, sim);
+                    births.push_back(d);
+                    ++tick_div;
+                }
+            } else if (ch.event == MARL_EVENT_DEATH) {
+                deaths.push_back(ch.cell);
+                ++tick_death;
+            }
+        }
+        total_div += tick_div;
+        total_death += tick_death;
+        // Deaths arrive in ascending cell order without duplicates (one event
+        // per cell); remove them back to front with swap_remove, tracking
+        // which original slot ends up in each hole.
+        const uint32_t n0 = (uint32_t)cells.size();
+        std::vector<uint32_t> origin(n0);
+        for (uint32_t i = 0; i < n0; ++i) origin[i] = i;
+        for (auto it = deaths.rbegin(); it != deaths.rend(); ++it) {
+            const uint32_t i = *it;
+            cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = -1;
+            cells[i] = cells.back();
+            origin[i] = origin[cells.size() - 1];
+            cells.pop_back();
+            if (i < cells.size()) cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = (int32_t)i;
+        }
+        const uint32_t n_after = (uint32_t)cells.size();
+        std::vector<uint32_t> mdst, msrc;
+        for (uint32_t d : deaths)
+            if (d < n_after && origin[d] != d) {
+                mdst.push_back(d);
+                msrc.push_back(origin[d]);
+            }
+        // Births append unless the voxel was taken meanwhile (lib.rs:270-277).
+        std::vector<marl_cell> accepted;
+        for (auto& b : births) {
+            const size_t v = vox(b.pos[0], b.pos[1], b.pos[2]);
+            if (cmap[v] < 0) {
+                cmap[v] = (int32_t)cells.size();
+                HostCell h;
+                std::memcpy(h.pos, b.pos, sizeof(h.pos));
+                h.starter_type = b.starter_type;
+                h.lineage_id = b.lineage_id;
+                h.ruleset = b.ruleset;
+                cells.push_back(h);
+                accepted.push_back(b);
+            }
+        }
+        marl_edit_list e;
+        e.n_halve = (uint32_t)halve.size();
+        e.halve = halve.data();
+        e.n_deaths = (uint32_t)deaths.size();
+        e.deaths = deaths.data();
+        e.n_moves = (uint32_t)mdst.size();
+        e.move_dst = mdst.data();
+        e.move_src = msrc.data();
+        e.n_after_deaths = n_after;
+        e.n_births = (uint32_t)accepted.size();
+        e.births = accepted.data();
+        return marl_apply_edits(ctx, &e);
+    }
+
+    marl_status step_once() {
+        uint32_t count = 0;
+        if (changes.size() < cells.size() + 1) changes.resize(cells.size() + 1);
+        marl_status st = marl_tick(ctx, changes.data(), (uint32_t)changes.size(), &count);
+        if (st) return st;
+        if ((st = process_changes(count))) return st;
+        ++tick;
+        return MARL_OK;
+    }
+};
+
+extern "C" {
+
+// Transfer counters are read from the context.
+uint64_t marl_internal_ctx_h2d(marl_ctx* c);
+uint64_t marl_internal_ctx_d2h(marl_ctx* c);
+
+static marl_status engine_init(marl_engine* e, int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
+                               uint64_t seed, uint32_t cap) {
+    e->X = gx, e->Y = gy, e->Z = gz;
+    e->sim = *sim;
+    e->rng.seed_with(seed);
+    e->cmap.assign((size_t)gx * gy * gz, -1);
+    return marl_ctx_create(gx, gy, gz, sim, cap, &e->ctx);
+}
+
+static marl_status engine_upload(marl_engine* e, const std::vector<float>& field, const std::vector<marl_cell>& cells) {
+    marl_status st = marl_upload_field(e->ctx, field.data());
+    if (st) return st;
+    return marl_upload_cells(e->ctx, cells.data(), (uint32_t)cells.size());
+}
+
+marl_status marl_engine_create(int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim, uint64_t rng_seed,
+                               uint32_t seed_count, uint32_t cell_capacity, marl_engine** out) {
+    if (!sim || !out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    *out = nullptr;
+    if (gx <= 2 * (int)sim->seed_margin || gy <= 2 * (int)sim->seed_margin)
+        return fail(MARL_ERR_INVALID_INPUT, "grid %dx%d too small for seed_margin %u", gx, gy, sim->seed_margin);
+    marl_engine* e = new (std::nothrow) marl_engine();
+    if (!e) return fail(MARL_ERR_OUT_OF_MEMORY, "host allocation");
+    marl_status st = engine_init(e, gx, gy, gz, sim, rng_seed, cell_capacity);
+    if (st) {
+        delete e;
+        return st;
+    }
+    // init_field_boundaries (crates/marl-sim/src/seeding.rs:9-26)
+    std::vector<float> field((size_t)gx * gy * gz * MARL_S_EXT, 0.0f);
+    const int layers = (int)sim->boundary_prime_layers;
+    for (int y = 0; y < gy; ++y)
+        for (int x = 0; x < gx; ++x) {
+            for (int z = 0; z < layers && z < gz; ++z) {
+                field[e->vox(x, y, z) * 12 + 1] = sim->boundary_prime_oxidant;
+                field[e->vox(x, y, z) * 12 + 3] = sim->boundary_prime_carbon;
+            }
+            for (int z = std::max(gz - layers, 0); z < gz; ++z) field[e->vox(x, y, z) * 12 + 2] = sim->boundary_prime_reductant;
+        }
+    // seed_cells x3 with depth bands scaled by Z/200 (lib.rs:59-105, seeding.rs:28-58)
+    std::vector<marl_cell> cells;
+    const float z_scale = (float)gz / 200.0f;
+    const float lo_f[3] = {sim->phototroph_z_lo, sim->chemolithotroph_z_lo, sim->anaerobe_z_lo};
+    const float hi_f[3] = {sim->phototroph_z_hi, sim->chemolithotroph_z_hi, sim->anaerobe_z_hi};
+    const float min_span[3] = {1.0f, 3.0f, 3.0f};
+    for (int kind = 0; kind < 3; ++kind) {
+        const uint16_t lo = (uint16_t)(lo_f[kind] * z_scale);
+        const uint16_t hi = (uint16_t)std::fmax(hi_f[kind] * z_scale, (float)lo + min_span[kind]);
+        const uint32_t zhi = std::min<uint32_t>(hi, (uint32_t)gz);
+        if (seed_count > 0 && lo >= zhi) {
+            marl_engine_destroy(e);
+            return fail(MARL_ERR_INVALID_INPUT, "empty seeding depth band [%u,%u)", lo, zhi);
+        }
+        uint32_t seeded = 0;
+        for (uint32_t a = 0; a < seed_count * 8 && seeded < seed_count; ++a) {
+            const uint16_t x = (uint16_t)e->rng.range(sim->seed_margin, (uint32_t)gx - sim->seed_margin);
+            const uint16_t y = (uint16_t)e->rng.range(sim->seed_margin, (uint32_t)gy - sim->seed_margin);
+            const uint16_t z = (uint16_t)e->rng.range(lo, zhi);
+            const size_t v = e->vox(x, y, z);
+            if (e->cmap[v] >= 0) continue;
+            const uint16_t pos[3] = {x, y, z};
+            const marl_cell c = starter(kind, pos, e->rng.u64());
+            e->cmap[v] = (int32_t)cells.size();
+            cells.push_back(c);
+            ++seeded;
+        }
+    }
+    if (cells.size() > cell_capacity) {
+        marl_engine_destroy(e);
+        return fail(MARL_ERR_CAPACITY, "%zu seeded cells exceed capacity %u", cells.size(), cell_capacity);
+    }
+    for (const auto& c : cells) {
+        HostCell h;
+        std::memcpy(h.pos, c.pos, sizeof(h.pos));
+        h.starter_type = c.starter_type;
+        h.lineage_id = c.lineage_id;
+        h.ruleset = c.ruleset;
+        e->cells.push_back(h);
+    }
+    if ((st = engine_upload(e, field, cells))) {
+        marl_engine_destroy(e);
+        return st;
+    }
+    *out = e;
+    return MARL_OK;
+}
+
+marl_status marl_engine_create_from_state(int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
+                                          uint64_t rng_seed, const float* field, const marl_cell* cells, uint32_t n,
+                                          uint32_t cell_capacity, marl_engine** out) {
+    if (!sim || !out || !field || (n && !cells)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    *out = nullptr;
+    marl_engine* e = new (std::nothrow) marl_engine();
+    if (!e) return fail(MARL_ERR_OUT_OF_MEMORY, "host allocation");
+    marl_status st = engine_init(e, gx, gy, gz, sim, rng_seed, cell_capacity);
+    if (st) {
+        delete e;
+        return st;
+    }
+    std::vector<float> f(field, field + (size_t)gx * gy * gz * MARL_S_EXT);
+    std::vector<marl_cell> cv(cells, cells + n);
+    if ((st = engine_upload(e, f, cv))) {  // validates positions
+        marl_engine_destroy(e);
+        return st;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        HostCell h;
+        std::memcpy(h.pos, cells[i].pos, sizeof(h.pos));
+        h.starter_type = cells[i].starter_type;
+        h.lineage_id = cells[i].lineage_id;
+        h.ruleset = cells[i].ruleset;
+        e->cells.push_back(h);
+        e->cmap[e->vox(h.pos[0], h.pos[1], h.pos[2])] = (int32_t)i;
+    }
+    *out = e;
+    return MARL_OK;
+}
+
+void marl_engine_destroy(marl_engine* e) {
+    if (!e) return;
+    if (e->ctx) marl_ctx_destroy(e->ctx);
+    delete e;
+}
+
+marl_status marl_engine_set_stream(marl_engine* e, void* stream) {
+    if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    return marl_ctx_set_stream(e->ctx, stream);
+}
+
+marl_status marl_engine_step(marl_engine* e, uint32_t ticks) {
+    if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    for (uint32_t t = 0; t < ticks; ++t) {
+        const uint64_t h0 = marl_internal_ctx_h2d(e->ctx), d0 = marl_internal_ctx_d2h(e->ctx);
+        marl_status st = e->step_once();
+        if (st) return st;
+        e->h2d_last = marl_internal_ctx_h2d(e->ctx) - h0;
+        e->d2h_last = marl_internal_ctx_d2h(e->ctx) - d0;
+    }
+    return MARL_OK;
+}
+
+marl_status marl_engine_stats_get(marl_engine* e, marl_engine_stats* s) {
+    if (!e || !s) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    s->tick = e->tick;
+    s->population = e->cells.size();
+    s->total_divisions = e->total_div;
+    s->total_deaths = e->total_death;
+    s->tick_divisions = e->tick_div;
+    s->tick_deaths = e->tick_death;
+    s->h2d_bytes_last_tick = e->h2d_last;
+    s->d2h_bytes_last_tick = e->d2h_last;
+    return MARL_OK;
+}
+
+marl_status marl_engine_get_cells(marl_engine* e, marl_cell* out, uint32_t cap, uint32_t* n_out) {
+    if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    return marl_download_cells(e->ctx, out, cap, n_out);
+}
+
+marl_status marl_engine_get_field(marl_engine* e, float* field) {
+    if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    return marl_download_field(e->ctx, field);
+}
+
+marl_status marl_engine_get_light(marl_engine* e, float* light) {
+    if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    return marl_download_light(e->ctx, light);
+}
+
+marl_ctx* marl_engine_ctx(marl_engine* e) { return e ? e->ctx : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// Internal host-side interface between the C-ABI layer (ctx.cu, engine.cpp)
+// and the kernel translation units (field.cu, cells.cu).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace marl {
+
+// Tensor maps and tile choice for the diffusion kernel over one pair of
+// ping-pong buffers and one occupancy mask.
+struct DiffusionPlan {
+    CUtensorMap tm_field[2];  // source = buffer 0 / buffer 1
+    CUtensorMap tm_mask;
+    int tile = 0;  // index into the tile-shape table
+    int zc = 16;   // z-chunk per CTA
+};
+
+int diffusion_tile_count();
+void diffusion_tile_shape(int tile, int* tx, int* ty);
+bool encode_field_map(CUtensorMap* m, const float* base, const Grid& g, int tx, int ty);
+bool encode_mask_map(CUtensorMap* m, const uint8_t* base, const Grid& g, int tx, int ty);
+bool plan_diffusion(DiffusionPlan* plan, const float* a, const float* b, const uint8_t* mask, const Grid& g,
+                    int tile, int zc);
+
+cudaError_t launch_sources(float* f, const Grid& g, const FieldConsts& k, cudaStream_t s);
+cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const float* src, float* dst, const Grid& g,
+                           const FieldConsts& k, int apply_sources, uint32_t* err, cudaStream_t s);
+cudaError_t launch_light(const float* f, const uint8_t* mask, float* light, const Grid& g, const FieldConsts& k,
+                         cudaStream_t s);
+cudaError_t launch_mass(const float* f, const Grid& g, double* partial, double* out, cudaStream_t s);
+size_t mass_partial_doubles();
+cudaError_t launch_repack_mask(const uint8_t* occ, uint8_t* mask, const Grid& g, cudaStream_t s);
+cudaError_t launch_unpack_mask(const uint8_t* mask, uint8_t* occ, const Grid& g, cudaStream_t s);
+
+// ---- cells ----
+struct ChangeHeader {  // device-written, read back with the change list
+    uint32_t count;     // Division + Death events this tick
+    uint32_t err;       // kErr* bits accumulated by kernels
+    uint32_t n_cells;
+    uint32_t pad[13];
+};
+static_assert(sizeof(ChangeHeader) == 64, "change header is 64 bytes");
+
+struct CellLaunch {
+    CellTable t;
+    uint32_t n;
+    Grid g;
+    const uint8_t* mask;
+    const int32_t* cmap;
+    float* field;
+    const float* light;
+    CellConsts k;
+    uint32_t epoch;
+    uint32_t* ticket;
+    uint32_t* err;
+};
+
+cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s);
+cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s);
+// Ordered compaction of Division/Death events into `changes` (after a
+// 64-byte ChangeHeader); block_counts needs compaction_blocks(n) words.
+uint32_t compaction_blocks(uint32_t n);
+cudaError_t launch_compact_events(const CellTable& t, uint32_t n, uint32_t* block_counts, ChangeHeader* hdr,
+                                  marl_change* changes, uint32_t cap, cudaStream_t s);
+
+cudaError_t launch_cells_from_records(const marl_cell* rec, uint32_t count, uint32_t base, CellTable t, const Grid& g,
+                                      int32_t* cmap, uint8_t* mask, uint32_t* err, cudaStream_t s);
+cudaError_t launch_cells_to_records(const CellTable& t, uint32_t n, marl_cell* rec, cudaStream_t s);
+cudaError_t launch_halve(const CellTable& t, const uint32_t* idx, uint32_t count, cudaStream_t s);
+cudaError_t launch_clear_dead(const CellTable& t, const uint32_t* idx, uint32_t count, const Grid& g, int32_t* cmap,
+                              uint8_t* mask, cudaStream_t s);
+cudaError_t launch_moves(CellTable t, const uint32_t* dst, const uint32_t* src, uint32_t count, const Grid& g,
+                         int32_t* cmap, cudaStream_t s);
+cudaError_t launch_rebuild_maps(const CellTable& t, uint32_t n, const Grid& g, int32_t* cmap, uint8_t* mask,
+                                cudaStream_t s);
+
+}  // namespace marl

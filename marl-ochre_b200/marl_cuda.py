@@ -1,0 +1,505 @@
+"""Python binding of libmarl_cuda.so (ctypes over the C ABI in include/marl_cuda.h).
+
+This is the host-side mirror of the reference's plugin seam for the per-tick
+field-and-cell path:
+
+* ``Context`` — device-resident field, light, occupancy and cell table, with
+  per-phase calls.  ``Context.diffuse_tick_with_cells`` is the counterpart of
+  ``GpuFieldDiffuser::diffuse_tick_with_cells``
+  (crates/marl-gpu/src/field_diffusion.rs:158-268): same arguments (a host
+  field, a host occupancy of one bool per voxel, the simulation config) and
+  the same error behaviour (invalid sizes -> ``MarlError`` with status
+  INVALID_INPUT, ``diffusion_substeps == 0`` -> no work).
+* ``Engine`` — the tick loop of ``marl_sim::run`` (crates/marl-sim/src/lib.rs:
+  160-277) with fate, division and mutation on the host.
+
+There is no CPU fallback: if the shared library or a CUDA device is missing,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int32, c_uint8, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+S_EXT = 12
+M_INT = 16
+R_MAX = 16
+NO_COFACTOR = 0xFF
+
+EVENT_NONE, EVENT_DIVISION, EVENT_DEATH, EVENT_QUIESCENCE = 0, 1, 2, 3
+SOURCES_ADDITIVE, SOURCES_DIRICHLET = 0, 1
+
+STATUS_NAMES = {
+    0: "OK",
+    1: "INVALID_INPUT",
+    2: "NO_DEVICE",
+    3: "CUDA",
+    4: "OUT_OF_MEMORY",
+    5: "TIMEOUT",
+    6: "CAPACITY",
+    7: "STATE",
+}
+
+# ---- plain-data layouts (must match include/marl_cuda.h) --------------------
+RECEPTOR_DTYPE = np.dtype([("k_half", "<f4"), ("n_hill", "<f4"), ("gain", "<f4")])
+TRANSPORT_DTYPE = np.dtype(
+    [("uptake_rate", "<f4"), ("secrete_rate", "<f4"), ("ext_species", "u1"), ("int_species", "u1"), ("_pad", "u1", (2,))]
+)
+REACTION_DTYPE = np.dtype(
+    [("substrate", "u1"), ("product", "u1"), ("catalyst", "u1"), ("cofactor", "u1"),
+     ("k_m", "<f4"), ("v_max", "<f4"), ("k_cat", "<f4")]
+)
+EFFECTOR_DTYPE = np.dtype(
+    [("threshold", "<f4"), ("rate", "<f4"), ("int_species", "u1"), ("ext_species", "u1"), ("_pad", "u1", (2,))]
+)
+FATE_DTYPE = np.dtype(
+    [("division_energy", "<f4"), ("death_energy", "<f4"), ("quiescence_energy", "<f4"), ("division_prep_ticks", "<f4")]
+)
+RULESET_DTYPE = np.dtype(
+    [("receptors", RECEPTOR_DTYPE, (8,)), ("transport", TRANSPORT_DTYPE, (8,)), ("reactions", REACTION_DTYPE, (16,)),
+     ("effectors", EFFECTOR_DTYPE, (8,)), ("fate", FATE_DTYPE), ("hgt_propensity", "<f4"), ("mutation_rate", "<f4")]
+)
+CELL_DTYPE = np.dtype(
+    [("pos", "<u2", (3,)), ("quiescent", "u1"), ("starter_type", "u1"), ("age", "<u4"), ("prep_remaining", "<u2"),
+     ("_pad0", "<u2"), ("lineage_id", "<u8"), ("internal", "<f4", (16,)), ("ruleset", RULESET_DTYPE)]
+)
+CHANGE_DTYPE = np.dtype(
+    [("cell", "<u4"), ("event", "u1"), ("quiescent", "u1"), ("_pad", "<u2"), ("internal", "<f4", (16,))]
+)
+assert RULESET_DTYPE.itemsize == 568 and CELL_DTYPE.itemsize == 656 and CHANGE_DTYPE.itemsize == 72
+
+
+class SimParams(ctypes.Structure):
+    """marl_sim_params == SimulationConfig (crates/marl-config/src/lib.rs:41-106)."""
+
+    _fields_ = [
+        ("dx", c_float), ("dt", c_float), ("diffusion_substeps", c_uint32),
+        ("d_voxel", c_float * S_EXT), ("lambda_decay", c_float * S_EXT),
+        ("source_rate_oxidant", c_float), ("source_rate_carbon", c_float), ("source_rate_reductant", c_float),
+        ("epsilon", c_float), ("c_max", c_float), ("lambda_maintenance", c_float), ("hard_death_floor", c_float),
+        ("reaction_maintenance", c_float), ("base_division_prep", c_float), ("prep_maintenance_multiplier", c_float),
+        ("rush_penalty_rate", c_float), ("alpha_eps", c_float), ("k_eps", c_float), ("light_efficiency", c_float),
+        ("surface_intensity", c_float), ("cell_absorption", c_float), ("chemical_absorption", c_float),
+        ("light_floor", c_float), ("mutation_stddev", c_float), ("structural_mutation_rate_mult", c_float),
+        ("meta_mutation_rate", c_float), ("meta_mutation_clamp_low", c_float), ("meta_mutation_clamp_high", c_float),
+        ("hill_exponent_clamp_low", c_float), ("hill_exponent_clamp_high", c_float),
+        ("active_reaction_threshold", c_float), ("seed_margin", c_uint32), ("phototroph_z_lo", c_float),
+        ("phototroph_z_hi", c_float), ("chemolithotroph_z_lo", c_float), ("chemolithotroph_z_hi", c_float),
+        ("anaerobe_z_lo", c_float), ("anaerobe_z_hi", c_float), ("division_neighbor_distance", c_uint32),
+        ("boundary_prime_layers", c_uint32), ("boundary_prime_oxidant", c_float),
+        ("boundary_prime_carbon", c_float), ("boundary_prime_reductant", c_float), ("source_mode", c_uint32),
+    ]
+
+    def copy(self) -> "SimParams":
+        out = SimParams()
+        ctypes.memmove(ctypes.byref(out), ctypes.byref(self), ctypes.sizeof(SimParams))
+        return out
+
+
+class EngineStats(ctypes.Structure):
+    _fields_ = [(name, c_uint64) for name in (
+        "tick", "population", "total_divisions", "total_deaths", "tick_divisions", "tick_deaths",
+        "h2d_bytes_last_tick", "d2h_bytes_last_tick")]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [("h2d_bytes", c_uint64), ("d2h_bytes", c_uint64), ("kernel_launches", c_uint64), ("ticks", c_uint64),
+                ("device_us", c_double)]
+
+
+class EditList(ctypes.Structure):
+    _fields_ = [
+        ("n_halve", c_uint32), ("halve", POINTER(c_uint32)),
+        ("n_deaths", c_uint32), ("deaths", POINTER(c_uint32)),
+        ("n_moves", c_uint32), ("move_dst", POINTER(c_uint32)), ("move_src", POINTER(c_uint32)),
+        ("n_after_deaths", c_uint32),
+        ("n_births", c_uint32), ("births", c_void_p),
+    ]
+
+
+class MarlError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str = ""):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{where}: {self.status_name} ({status}) {message}".strip())
+
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmarl_cuda.so")
+
+# Every symbol declared in include/marl_cuda.h (checked by tests against the header).
+EXPORTED = [
+    "marl_sim_params_default", "marl_last_error", "marl_abi_version",
+    "marl_ctx_create", "marl_ctx_destroy", "marl_ctx_set_stream", "marl_ctx_set_params", "marl_ctx_synchronize",
+    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_autotune", "marl_ctx_counters",
+    "marl_upload_field", "marl_download_field", "marl_upload_light", "marl_download_light",
+    "marl_upload_cells", "marl_download_cells", "marl_cell_count", "marl_download_occupancy",
+    "marl_apply_boundary_sources", "marl_diffuse", "marl_light_update", "marl_cell_phase", "marl_tick",
+    "marl_apply_edits", "marl_mass_f64", "marl_diffuse_tick_with_cells", "marl_diffuse_device",
+    "marl_ruleset_pack_canonical", "marl_ruleset_unpack_canonical",
+    "marl_engine_create", "marl_engine_create_from_state", "marl_engine_destroy", "marl_engine_set_stream",
+    "marl_engine_step", "marl_engine_stats_get", "marl_engine_get_cells", "marl_engine_get_field",
+    "marl_engine_get_light", "marl_engine_ctx",
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libmarl_cuda.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built; run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    P = c_void_p
+    sig = {
+        "marl_sim_params_default": (c_int32, [POINTER(SimParams)]),
+        "marl_last_error": (c_char_p, []),
+        "marl_abi_version": (c_uint32, []),
+        "marl_ctx_create": (c_int32, [c_int32, c_int32, c_int32, POINTER(SimParams), c_uint32, POINTER(c_void_p)]),
+        "marl_ctx_destroy": (None, [P]),
+        "marl_ctx_set_stream": (c_int32, [P, P]),
+        "marl_ctx_set_params": (c_int32, [P, POINTER(SimParams)]),
+        "marl_ctx_synchronize": (c_int32, [P]),
+        "marl_ctx_set_tile": (c_int32, [P, c_int32, c_int32]),
+        "marl_ctx_get_tile": (c_int32, [P, POINTER(c_int32), POINTER(c_int32)]),
+        "marl_ctx_autotune": (c_int32, [P, c_int32, POINTER(c_float)]),
+        "marl_ctx_counters": (c_int32, [P, POINTER(Counters)]),
+        "marl_upload_field": (c_int32, [P, P]),
+        "marl_download_field": (c_int32, [P, P]),
+        "marl_upload_light": (c_int32, [P, P]),
+        "marl_download_light": (c_int32, [P, P]),
+        "marl_upload_cells": (c_int32, [P, P, c_uint32]),
+        "marl_download_cells": (c_int32, [P, P, c_uint32, POINTER(c_uint32)]),
+        "marl_cell_count": (c_int32, [P, POINTER(c_uint32)]),
+        "marl_download_occupancy": (c_int32, [P, P]),
+        "marl_apply_boundary_sources": (c_int32, [P]),
+        "marl_diffuse": (c_int32, [P, c_uint32, c_int32]),
+        "marl_light_update": (c_int32, [P]),
+        "marl_cell_phase": (c_int32, [P, P]),
+        "marl_tick": (c_int32, [P, P, c_uint32, POINTER(c_uint32)]),
+        "marl_apply_edits": (c_int32, [P, POINTER(EditList)]),
+        "marl_mass_f64": (c_int32, [P, P]),
+        "marl_diffuse_tick_with_cells": (c_int32, [P, P, P]),
+        "marl_diffuse_device": (c_int32, [P, P, P, c_int32, c_int32, c_int32, POINTER(SimParams), c_uint32, P]),
+        "marl_ruleset_pack_canonical": (c_int32, [P, P]),
+        "marl_ruleset_unpack_canonical": (c_int32, [P, P]),
+        "marl_engine_create": (c_int32, [c_int32, c_int32, c_int32, POINTER(SimParams), c_uint64, c_uint32, c_uint32,
+                                         POINTER(c_void_p)]),
+        "marl_engine_create_from_state": (c_int32, [c_int32, c_int32, c_int32, POINTER(SimParams), c_uint64, P, P,
+                                                    c_uint32, c_uint32, POINTER(c_void_p)]),
+        "marl_engine_destroy": (None, [P]),
+        "marl_engine_set_stream": (c_int32, [P, P]),
+        "marl_engine_step": (c_int32, [P, c_uint32]),
+        "marl_engine_stats_get": (c_int32, [P, POINTER(EngineStats)]),
+        "marl_engine_get_cells": (c_int32, [P, P, c_uint32, POINTER(c_uint32)]),
+        "marl_engine_get_field": (c_int32, [P, P]),
+        "marl_engine_get_light": (c_int32, [P, P]),
+        "marl_engine_ctx": (c_void_p, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int, where: str) -> None:
+    if status != 0:
+        msg = _lib.marl_last_error().decode(errors="replace") if _lib is not None else ""
+        raise MarlError(status, where, msg)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def default_params() -> SimParams:
+    """SimulationConfig::default() (crates/marl-config/src/lib.rs:108-168)."""
+    lib = load()
+    p = SimParams()
+    _check(lib.marl_sim_params_default(ctypes.byref(p)), "marl_sim_params_default")
+    return p
+
+
+def _as_field(field: np.ndarray, dims) -> np.ndarray:
+    X, Y, Z = dims
+    if field.dtype != np.float32 or field.size != X * Y * Z * S_EXT or not field.flags.c_contiguous:
+        raise MarlError(1, "field", f"expected contiguous float32 with {X * Y * Z * S_EXT} values")
+    return field
+
+
+class Context:
+    """Device-resident state for one grid (marl_ctx)."""
+
+    def __init__(self, dims, params: SimParams | None = None, cell_capacity: int = 1 << 16):
+        self.lib = load()
+        self.dims = tuple(int(d) for d in dims)
+        self.params = (params or default_params()).copy()
+        h = c_void_p()
+        X, Y, Z = self.dims
+        _check(self.lib.marl_ctx_create(X, Y, Z, ctypes.byref(self.params), cell_capacity, ctypes.byref(h)),
+               "marl_ctx_create")
+        self.h = h
+        self.cell_capacity = cell_capacity
+
+    # lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.marl_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def voxels(self) -> int:
+        X, Y, Z = self.dims
+        return X * Y * Z
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib.marl_ctx_set_stream(self.h, c_void_p(stream_ptr)), "marl_ctx_set_stream")
+
+    def set_params(self, params: SimParams) -> None:
+        self.params = params.copy()
+        _check(self.lib.marl_ctx_set_params(self.h, ctypes.byref(self.params)), "marl_ctx_set_params")
+
+    def synchronize(self) -> None:
+        _check(self.lib.marl_ctx_synchronize(self.h), "marl_ctx_synchronize")
+
+    def set_tile(self, tile: int, zc: int) -> None:
+        _check(self.lib.marl_ctx_set_tile(self.h, tile, zc), "marl_ctx_set_tile")
+
+    def get_tile(self) -> tuple[int, int]:
+        t, z = c_int32(), c_int32()
+        _check(self.lib.marl_ctx_get_tile(self.h, ctypes.byref(t), ctypes.byref(z)), "marl_ctx_get_tile")
+        return t.value, z.value
+
+    def autotune(self, reps: int = 5) -> float:
+        """Pick the fastest diffusion tile shape / z-chunk; returns us per substep."""
+        us = c_float()
+        _check(self.lib.marl_ctx_autotune(self.h, reps, ctypes.byref(us)), "marl_ctx_autotune")
+        return us.value
+
+    def counters(self) -> dict:
+        c = Counters()
+        _check(self.lib.marl_ctx_counters(self.h, ctypes.byref(c)), "marl_ctx_counters")
+        return {name: getattr(c, name) for name, _ in Counters._fields_}
+
+    # state transfer
+    def upload_field(self, field: np.ndarray) -> None:
+        f = _as_field(np.ascontiguousarray(field, dtype=np.float32), self.dims)
+        _check(self.lib.marl_upload_field(self.h, _ptr(f)), "marl_upload_field")
+
+    def download_field(self) -> np.ndarray:
+        X, Y, Z = self.dims
+        out = np.empty((Z, Y, X, S_EXT), np.float32)
+        _check(self.lib.marl_download_field(self.h, _ptr(out)), "marl_download_field")
+        return out
+
+    def upload_light(self, light: np.ndarray) -> None:
+        l = np.ascontiguousarray(light, dtype=np.float32)
+        if l.size != self.voxels:
+            raise MarlError(1, "upload_light", "size mismatch")
+        _check(self.lib.marl_upload_light(self.h, _ptr(l)), "marl_upload_light")
+
+    def download_light(self) -> np.ndarray:
+        X, Y, Z = self.dims
+        out = np.empty((Z, Y, X), np.float32)
+        _check(self.lib.marl_download_light(self.h, _ptr(out)), "marl_download_light")
+        return out
+
+    def upload_cells(self, cells: np.ndarray) -> None:
+        c = np.ascontiguousarray(cells, dtype=CELL_DTYPE)
+        _check(self.lib.marl_upload_cells(self.h, _ptr(c) if c.size else None, c.size), "marl_upload_cells")
+
+    def cell_count(self) -> int:
+        n = c_uint32()
+        _check(self.lib.marl_cell_count(self.h, ctypes.byref(n)), "marl_cell_count")
+        return n.value
+
+    def download_cells(self) -> np.ndarray:
+        n = self.cell_count()
+        out = np.zeros(max(n, 1), CELL_DTYPE)
+        got = c_uint32()
+        _check(self.lib.marl_download_cells(self.h, _ptr(out), out.size, ctypes.byref(got)), "marl_download_cells")
+        return out[: got.value]
+
+    def download_occupancy(self) -> np.ndarray:
+        X, Y, Z = self.dims
+        out = np.empty((Z, Y, X), np.uint8)
+        _check(self.lib.marl_download_occupancy(self.h, _ptr(out)), "marl_download_occupancy")
+        return out
+
+    # phases
+    def apply_boundary_sources(self) -> None:
+        _check(self.lib.marl_apply_boundary_sources(self.h), "marl_apply_boundary_sources")
+
+    def diffuse(self, substeps: int | None = None, fuse_sources: bool = False) -> None:
+        s = self.params.diffusion_substeps if substeps is None else substeps
+        _check(self.lib.marl_diffuse(self.h, s, 1 if fuse_sources else 0), "marl_diffuse")
+
+    def light_update(self) -> None:
+        _check(self.lib.marl_light_update(self.h), "marl_light_update")
+
+    def cell_phase(self) -> np.ndarray:
+        n = self.cell_count()
+        ev = np.zeros(max(n, 1), np.uint8)
+        _check(self.lib.marl_cell_phase(self.h, _ptr(ev)), "marl_cell_phase")
+        return ev[:n]
+
+    def tick(self, cap: int | None = None) -> np.ndarray:
+        cap = self.cell_capacity if cap is None else cap
+        out = np.zeros(max(cap, 1), CHANGE_DTYPE)
+        n = c_uint32()
+        _check(self.lib.marl_tick(self.h, _ptr(out), cap, ctypes.byref(n)), "marl_tick")
+        return out[: n.value]
+
+    def apply_edits(self, halve=(), deaths=(), moves=(), n_after_deaths=None, births=None) -> None:
+        halve = np.ascontiguousarray(halve, np.uint32)
+        deaths = np.ascontiguousarray(deaths, np.uint32)
+        moves = np.asarray(moves, np.uint32).reshape(-1, 2)
+        dst = np.ascontiguousarray(moves[:, 0])
+        src = np.ascontiguousarray(moves[:, 1])
+        births = np.zeros(0, CELL_DTYPE) if births is None else np.ascontiguousarray(births, CELL_DTYPE)
+        if n_after_deaths is None:
+            n_after_deaths = self.cell_count() - deaths.size
+        u32p = POINTER(c_uint32)
+        e = EditList(
+            halve.size, halve.ctypes.data_as(u32p), deaths.size, deaths.ctypes.data_as(u32p),
+            dst.size, dst.ctypes.data_as(u32p), src.ctypes.data_as(u32p), int(n_after_deaths),
+            births.size, births.ctypes.data if births.size else None,
+        )
+        _check(self.lib.marl_apply_edits(self.h, ctypes.byref(e)), "marl_apply_edits")
+
+    def mass_f64(self) -> np.ndarray:
+        out = np.zeros(S_EXT, np.float64)
+        _check(self.lib.marl_mass_f64(self.h, _ptr(out)), "marl_mass_f64")
+        return out
+
+    def diffuse_tick_with_cells(self, field: np.ndarray, occupancy: np.ndarray) -> None:
+        """GpuFieldDiffuser::diffuse_tick_with_cells: `field` is updated in place."""
+        X, Y, Z = self.dims
+        if field.dtype != np.float32 or field.size != X * Y * Z * S_EXT or not field.flags.c_contiguous:
+            raise MarlError(1, "diffuse_tick_with_cells",
+                            f"field has {field.size} floats, expected {X * Y * Z * S_EXT}")
+        occ = np.ascontiguousarray(occupancy).astype(np.uint8, copy=False)
+        if occ.size != X * Y * Z:
+            raise MarlError(1, "diffuse_tick_with_cells", f"occupancy has {occ.size} voxels, expected {X * Y * Z}")
+        _check(self.lib.marl_diffuse_tick_with_cells(self.h, _ptr(field), _ptr(occ)), "marl_diffuse_tick_with_cells")
+
+
+def diffuse_device(field_ptr: int, scratch_ptr: int, occ_ptr: int, dims, params: SimParams, substeps: int,
+                   stream_ptr: int = 0) -> None:
+    """marl_diffuse_device on caller-owned device buffers (raw pointers)."""
+    lib = load()
+    X, Y, Z = dims
+    _check(lib.marl_diffuse_device(c_void_p(field_ptr), c_void_p(scratch_ptr), c_void_p(occ_ptr), X, Y, Z,
+                                   ctypes.byref(params), substeps, c_void_p(stream_ptr)), "marl_diffuse_device")
+
+
+def pack_ruleset(rs: np.ndarray) -> bytes:
+    lib = load()
+    r = np.ascontiguousarray(rs, RULESET_DTYPE).reshape(1)
+    out = np.zeros(536, np.uint8)
+    _check(lib.marl_ruleset_pack_canonical(_ptr(r), _ptr(out)), "marl_ruleset_pack_canonical")
+    return out.tobytes()
+
+
+def unpack_ruleset(payload: bytes) -> np.ndarray:
+    lib = load()
+    buf = np.frombuffer(payload, np.uint8).copy()
+    if buf.size != 536:
+        raise MarlError(1, "unpack_ruleset", "payload must be 536 bytes")
+    out = np.zeros(1, RULESET_DTYPE)
+    _check(lib.marl_ruleset_unpack_canonical(_ptr(buf), _ptr(out)), "marl_ruleset_unpack_canonical")
+    return out[0]
+
+
+class Engine:
+    """marl_sim::run's tick loop (seeding, device tick, host fate) — marl_engine."""
+
+    def __init__(self, dims, params: SimParams | None = None, rng_seed: int = 42, seed_count: int = 30,
+                 cell_capacity: int = 1 << 18, field: np.ndarray | None = None, cells: np.ndarray | None = None):
+        self.lib = load()
+        self.dims = tuple(int(d) for d in dims)
+        self.params = (params or default_params()).copy()
+        X, Y, Z = self.dims
+        h = c_void_p()
+        if field is None:
+            _check(self.lib.marl_engine_create(X, Y, Z, ctypes.byref(self.params), rng_seed, seed_count,
+                                               cell_capacity, ctypes.byref(h)), "marl_engine_create")
+        else:
+            f = _as_field(np.ascontiguousarray(field, np.float32), self.dims)
+            c = np.ascontiguousarray(cells if cells is not None else np.zeros(0, CELL_DTYPE), CELL_DTYPE)
+            _check(self.lib.marl_engine_create_from_state(X, Y, Z, ctypes.byref(self.params), rng_seed, _ptr(f),
+                                                          _ptr(c) if c.size else None, c.size, cell_capacity,
+                                                          ctypes.byref(h)), "marl_engine_create_from_state")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.marl_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib.marl_engine_set_stream(self.h, c_void_p(stream_ptr)), "marl_engine_set_stream")
+
+    def counters(self) -> dict:
+        c = Counters()
+        _check(self.lib.marl_ctx_counters(self.lib.marl_engine_ctx(self.h), ctypes.byref(c)), "marl_ctx_counters")
+        return {name: getattr(c, name) for name, _ in Counters._fields_}
+
+    def autotune(self, reps: int = 5) -> float:
+        us = c_float()
+        _check(self.lib.marl_ctx_autotune(self.lib.marl_engine_ctx(self.h), reps, ctypes.byref(us)),
+               "marl_ctx_autotune")
+        return us.value
+
+    def step(self, ticks: int = 1) -> None:
+        _check(self.lib.marl_engine_step(self.h, ticks), "marl_engine_step")
+
+    def stats(self) -> dict:
+        s = EngineStats()
+        _check(self.lib.marl_engine_stats_get(self.h, ctypes.byref(s)), "marl_engine_stats_get")
+        return {name: getattr(s, name) for name, _ in EngineStats._fields_}
+
+    def cells(self) -> np.ndarray:
+        n = self.stats()["population"]
+        out = np.zeros(max(int(n), 1), CELL_DTYPE)
+        got = c_uint32()
+        _check(self.lib.marl_engine_get_cells(self.h, _ptr(out), out.size, ctypes.byref(got)), "marl_engine_get_cells")
+        return out[: got.value]
+
+    def field(self) -> np.ndarray:
+        X, Y, Z = self.dims
+        out = np.empty((Z, Y, X, S_EXT), np.float32)
+        _check(self.lib.marl_engine_get_field(self.h, _ptr(out)), "marl_engine_get_field")
+        return out
+
+    def light(self) -> np.ndarray:
+        X, Y, Z = self.dims
+        out = np.empty((Z, Y, X), np.float32)
+        _check(self.lib.marl_engine_get_light(self.h, _ptr(out)), "marl_engine_get_light")
+        return out
