@@ -206,7 +206,7 @@ def diffusion_roofline(marl, torch, engine, stream) -> dict:
     if traffic and traffic.get("grid") == list(DIMS):
         tr = traffic.get("dram_bytes_per_launch")
     ctx.close()
-    tiles = ["32x8", "32x4", "64x4", "16x16"]
+    tiles = ["16x8", "16x16", "16x4", "16x32"]
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tr, "kernel": "k_diffuse (diffusion substep, TMA z-march)", "peak_source": src,
             "algorithmic_bytes_per_launch": bytes_per_launch, "us_per_launch": t_sub * 1e6,
@@ -241,7 +241,9 @@ def main() -> int:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    stream = torch.cuda.current_stream()
+    # One explicit stream for the engine, the L2 flush and the timing events.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     eng = marl.Engine(DIMS, marl.default_params(), rng_seed=SEED, seed_count=SEED_COUNT, cell_capacity=1 << 20)
     eng.set_stream(stream.cuda_stream)

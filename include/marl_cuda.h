@@ -228,6 +228,8 @@ uint32_t marl_abi_version(void);
 marl_status marl_ctx_create(int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
                             uint32_t cell_capacity, marl_ctx** out);
 void marl_ctx_destroy(marl_ctx* ctx);
+/* All later work of the context is ordered on `cuda_stream` (a cudaStream_t;
+ * NULL = the legacy default stream).  A context starts on a stream of its own. */
 marl_status marl_ctx_set_stream(marl_ctx* ctx, void* cuda_stream);
 marl_status marl_ctx_set_params(marl_ctx* ctx, const marl_sim_params* sim);
 /* Waits for the context's stream and reports device-side errors. */

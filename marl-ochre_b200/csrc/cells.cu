@@ -60,11 +60,33 @@ __global__ void k_cell_schedule(CellTable t, uint32_t n, Grid g, const int32_t* 
 // ------------------------------------------------------------ update -----
 constexpr int kTickThreads = 128;
 
-struct CellScratch {  // per-thread arrays indexed dynamically: [k][thread]
+// Per-thread staging, [item][thread] so that dynamic indices never cause bank
+// conflicts: the cell's ruleset and internal state are copied in with cp.async
+// (independent loads in flight together) while the neighbour gather runs.
+struct CellScratch {
+    uint4 rx[MARL_R_MAX][kTickThreads];
+    float2 tp[MARL_S_TRANSPORTERS][kTickThreads];
+    float2 ef[MARL_S_EFFECTORS][kTickThreads];
+    uint4 idx[2][kTickThreads];  // transporter pairs, effector pairs
+    float4 fate[kTickThreads];
     float x[MARL_M_INT][kTickThreads];
     float ext[MARL_S_EXT][kTickThreads];
     float del[MARL_S_EXT][kTickThreads];
 };
+constexpr int kTickSmem = (int)sizeof(CellScratch);
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ void st4(float* p, float4 v) { __stcg(reinterpret_cast<float4*>(p), v); }
@@ -87,6 +109,21 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
                               -(long long)g.X * g.Y};
     const int n = __popc(nb);
 
+    // Stage the ruleset and internal state (asynchronous copies).
+#pragma unroll
+    for (int r = 0; r < MARL_R_MAX; ++r) cp_async16(&S.rx[r][tid], &t.rx[r * cap + j]);
+#pragma unroll
+    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) cp_async8(&S.tp[i][tid], &t.tp_rate[i * cap + j]);
+#pragma unroll
+    for (int i = 0; i < MARL_S_EFFECTORS; ++i) cp_async8(&S.ef[i][tid], &t.ef_par[i * cap + j]);
+    cp_async16(&S.idx[0][tid], &t.tp_idx[j]);
+    cp_async16(&S.idx[1][tid], &t.ef_idx[j]);
+    cp_async16(&S.fate[tid], &t.fate[j]);
+#pragma unroll
+    for (int k = 0; k < MARL_M_INT; ++k) cp_async4(&S.x[k][tid], &t.internal[k * cap + j]);
+    const uint32_t st0 = t.state[j];
+    const float light = a.light[vox];
+
     // Gather: mean of the empty face neighbours (spatial.rs:56-77).
 #pragma unroll
     for (int s = 0; s < 12; ++s) S.ext[s][tid] = 0.0f;
@@ -107,21 +144,20 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
     // CellState::tick (cell.rs:193-369).  Phase 1 (receptors) only writes an
     // unused local and is omitted.
 #pragma unroll
-    for (int k = 0; k < MARL_M_INT; ++k) S.x[k][tid] = t.internal[k * cap + j];
-#pragma unroll
     for (int s = 0; s < 12; ++s) S.del[s][tid] = 0.0f;
     const CellConsts& c = a.k;
     const float dt = c.dt;
+    cp_async_wait_all();
 
     // Phase 2: transport (cell.rs:223-238)
-    const uint4 tpi = t.tp_idx[j];
+    const uint4 tpi = S.idx[0][tid];
     const uint32_t tpw[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
         const uint32_t pair = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
         const uint32_t e = pair & 0xFF, k = pair >> 8;
         if (e >= MARL_S_EXT || k >= MARL_M_INT) continue;
-        const float2 r = t.tp_rate[i * cap + j];
+        const float2 r = S.tp[i][tid];
         const float ev = S.ext[e][tid];
         const float xk = S.x[k][tid];
         const float uptake = r.x * ev / (1.0f + ev);
@@ -129,14 +165,14 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
         S.x[k][tid] = rclamp(xk + (uptake - secretion) * dt, 0.0f, c.c_max);
         S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
     }
-    S.x[MARL_M_INT - 1][tid] = a.light[vox];  // cell.rs:243
+    S.x[MARL_M_INT - 1][tid] = light;  // cell.rs:243
 
     // Phase 3: reactions, strictly in slot order (cell.rs:246-285)
     const float feps = 1.1920928955078125e-07f;
     int active = 0;
 #pragma unroll 4
     for (int r = 0; r < MARL_R_MAX; ++r) {
-        const uint4 q = t.rx[r * cap + j];
+        const uint4 q = S.rx[r][tid];
         const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF, ci = (q.x >> 16) & 0xFF, fi = q.x >> 24;
         const float km = __uint_as_float(q.y), vmax = __uint_as_float(q.z), kcat = __uint_as_float(q.w);
         if (fabsf(vmax) > c.thr && si != pi) ++active;
@@ -160,10 +196,10 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
     }
 
     // Maintenance (cell.rs:291-311)
-    uint32_t st = t.state[j];
+    const uint32_t st = st0;
     uint32_t prep = st & 0xFFFFu;
     uint32_t quiescent = (st >> 16) & 1u;
-    const float4 fate = t.fate[j];
+    const float4 fate = S.fate[tid];
     float pm;
     if (prep > 0) {
         const float evolved = fmaxf(fate.w, 1.0f);
@@ -179,14 +215,14 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
 
     // Phase 4: effectors (cell.rs:314-329)
     if (!quiescent) {
-        const uint4 efi = t.ef_idx[j];
+        const uint4 efi = S.idx[1][tid];
         const uint32_t efw[4] = {efi.x, efi.y, efi.z, efi.w};
 #pragma unroll
         for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
             const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
             const uint32_t k = pair & 0xFF, e = pair >> 8;
             if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
-            const float2 pr = t.ef_par[i * cap + j];
+            const float2 pr = S.ef[i][tid];
             const float xk = S.x[k][tid];
             if (xk > pr.x) {
                 const float amount = pr.y * xk / (1.0f + xk) * dt;
@@ -249,7 +285,8 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
 }
 
 __global__ void __launch_bounds__(kTickThreads) k_cell_tick(CellLaunch a) {
-    __shared__ CellScratch S;
+    extern __shared__ __align__(16) unsigned char tick_smem[];
+    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const CellTable& t = a.t;
@@ -522,24 +559,38 @@ __global__ void k_clear_dead(CellTable t, const uint32_t* __restrict__ idx, uint
 // copies are independent.
 __global__ void k_moves(CellTable t, const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t count,
                         Grid g, int32_t* __restrict__ cmap) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // One warp per move; each lane copies a few words, all loads first.
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int l = threadIdx.x & 31;
     if (i >= count) return;
     const uint32_t d = dst[i], s = src[i];
     const size_t cap = t.cap;
-    t.pos[d] = t.pos[s];
-    t.age[d] = t.age[s];
-    t.state[d] = t.state[s];
-    t.lineage[d] = t.lineage[s];
-    for (int k = 0; k < MARL_M_INT; ++k) t.internal[k * cap + d] = t.internal[k * cap + s];
-    for (int k = 0; k < MARL_S_TRANSPORTERS; ++k) t.tp_rate[k * cap + d] = t.tp_rate[k * cap + s];
-    t.tp_idx[d] = t.tp_idx[s];
-    for (int k = 0; k < MARL_R_MAX; ++k) t.rx[k * cap + d] = t.rx[k * cap + s];
-    for (int k = 0; k < MARL_S_EFFECTORS; ++k) t.ef_par[k * cap + d] = t.ef_par[k * cap + s];
-    t.ef_idx[d] = t.ef_idx[s];
-    t.fate[d] = t.fate[s];
-    for (int k = 0; k < kColdFloats; ++k) t.cold[(size_t)d * kColdFloats + k] = t.cold[(size_t)s * kColdFloats + k];
-    const uint32_t P = t.pos[s];
-    cmap[((size_t)pos_z(P) * g.Y + pos_y(P)) * g.X + pos_x(P)] = (int32_t)d;
+    uint4 rx = make_uint4(0, 0, 0, 0);
+    float in = 0.0f, cold = 0.0f;
+    float2 tp = make_float2(0, 0), ef = make_float2(0, 0);
+    if (l < MARL_R_MAX) rx = t.rx[l * cap + s], in = t.internal[l * cap + s];
+    if (l < MARL_S_TRANSPORTERS) tp = t.tp_rate[l * cap + s], ef = t.ef_par[l * cap + s];
+    if (l < kColdFloats) cold = t.cold[(size_t)s * kColdFloats + l];
+    uint32_t pos = 0, age = 0, state = 0;
+    uint64_t lineage = 0;
+    uint4 w = make_uint4(0, 0, 0, 0);
+    float4 fate = make_float4(0, 0, 0, 0);
+    if (l == 26) pos = t.pos[s], age = t.age[s];
+    if (l == 27) state = t.state[s], lineage = t.lineage[s];
+    if (l == 28) w = t.tp_idx[s];
+    if (l == 29) w = t.ef_idx[s];
+    if (l == 30) fate = t.fate[s];
+    if (l < MARL_R_MAX) t.rx[l * cap + d] = rx, t.internal[l * cap + d] = in;
+    if (l < MARL_S_TRANSPORTERS) t.tp_rate[l * cap + d] = tp, t.ef_par[l * cap + d] = ef;
+    if (l < kColdFloats) t.cold[(size_t)d * kColdFloats + l] = cold;
+    if (l == 26) {
+        t.pos[d] = pos, t.age[d] = age;
+        cmap[((size_t)pos_z(pos) * g.Y + pos_y(pos)) * g.X + pos_x(pos)] = (int32_t)d;
+    }
+    if (l == 27) t.state[d] = state, t.lineage[d] = lineage;
+    if (l == 28) t.tp_idx[d] = w;
+    if (l == 29) t.ef_idx[d] = w;
+    if (l == 30) t.fate[d] = fate;
 }
 
 __global__ void k_rebuild_maps(CellTable t, uint32_t n, Grid g, int32_t* __restrict__ cmap,
@@ -563,11 +614,16 @@ cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s) {
 
 cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick, kTickThreads, 0);
+    static int per_sm = 0, configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e = cudaFuncSetAttribute(k_cell_tick, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick, kTickThreads, kTickSmem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
+        configured_device = dev;
     }
     const uint32_t warps_needed = (a.n + 31) / 32;
     const uint32_t blocks_needed = (warps_needed + (kTickThreads / 32) - 1) / (kTickThreads / 32);
@@ -575,7 +631,7 @@ cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
     // ticket holder is running (the dependency waits rely on it).
     const uint32_t resident = (uint32_t)per_sm * (uint32_t)num_sms;
     const uint32_t blocks = blocks_needed < resident ? blocks_needed : resident;
-    k_cell_tick<<<blocks, kTickThreads, 0, s>>>(a);
+    k_cell_tick<<<blocks, kTickThreads, kTickSmem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -618,7 +674,7 @@ cudaError_t launch_clear_dead(const CellTable& t, const uint32_t* idx, uint32_t 
 cudaError_t launch_moves(CellTable t, const uint32_t* dst, const uint32_t* src, uint32_t count, const Grid& g,
                          int32_t* cmap, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    k_moves<<<blocks_for(count, 128), 128, 0, s>>>(t, dst, src, count, g, cmap);
+    k_moves<<<blocks_for((size_t)count * 32, 128), 128, 0, s>>>(t, dst, src, count, g, cmap);
     return cudaGetLastError();
 }
 

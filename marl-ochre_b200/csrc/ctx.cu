@@ -143,7 +143,7 @@ static cudaError_t alloc_table(CellTable& t, uint32_t cap) {
 void ctx_free(marl_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* dev[] = {c->field[0], c->field[1], c->mask, c->cmap, c->light, c->d_hdr, c->d_changes, c->d_block_counts,
+    void* dev[] = {c->field[0], c->field[1], c->mask, c->cmap, c->light, c->c4, c->d_hdr, c->d_changes, c->d_block_counts,
                    c->d_edit, c->d_mass_partial, c->d_mass_out, c->d_records, c->d_occ_stage, c->d_seam_mask,
                    c->d_events_stage};
     for (void* p : dev)
@@ -207,7 +207,11 @@ CellLaunch cell_launch(marl_ctx* c) {
     return a;
 }
 
-marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources) {
+// `substeps` substeps; with emit_c4 the last one also writes species 4
+// compactly into c->c4 for the light scan (returns whether it did).
+marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources, bool emit_c4 = false,
+                            bool* c4_written = nullptr) {
+    if (c4_written) *c4_written = false;
     if (substeps == 0) {
         if (fuse_sources) {
             CK(launch_sources(c->field[c->cur], c->g, c->fk, c->stream));
@@ -216,10 +220,12 @@ marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources) {
         return MARL_OK;
     }
     for (uint32_t i = 0; i < substeps; ++i) {
-        CK(launch_diffuse(c->plan, c->cur, c->field[c->cur], c->field[c->cur ^ 1], c->g, c->fk,
-                          (fuse_sources && i == 0) ? 1 : 0, &c->d_hdr->err, c->stream));
+        float* c4 = (emit_c4 && i + 1 == substeps) ? c->c4 : nullptr;
+        CK(launch_diffuse(c->plan, c->cur, c->g, c->fk, (fuse_sources && i == 0) ? 1 : 0, c4, &c->d_hdr->err,
+                          c->stream));
         c->cur ^= 1;
         ++c->launches;
+        if (c4 && c4_written) *c4_written = true;
     }
     return MARL_OK;
 }
@@ -383,6 +389,7 @@ marl_status marl_ctx_create(int32_t gx, int32_t gy, int32_t gz, const marl_sim_p
     step(cudaMalloc((void**)&c->mask, (size_t)gz * gy * mask_pitch(gx)));
     step(cudaMalloc((void**)&c->cmap, V * 4));
     step(cudaMalloc((void**)&c->light, V * 4));
+    step(cudaMalloc((void**)&c->c4, V * 4));
     step(cudaMalloc((void**)&c->d_hdr, sizeof(ChangeHeader)));
     step(cudaMallocHost((void**)&c->h_hdr, sizeof(ChangeHeader) + (size_t)kPrefetchChanges * sizeof(marl_change)));
     step(cudaMalloc((void**)&c->d_changes, (size_t)cell_capacity * sizeof(marl_change)));
@@ -429,13 +436,9 @@ marl_status marl_ctx_set_stream(marl_ctx* c, void* stream) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
     CK(cudaStreamSynchronize(c->stream));
     if (c->own_stream) CK(cudaStreamDestroy(c->stream));
-    if (stream) {
-        c->stream = (cudaStream_t)stream;
-        c->own_stream = false;
-    } else {
-        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-        c->own_stream = true;
-    }
+    // NULL is the legacy default stream (what torch reports as stream 0).
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
     return MARL_OK;
 }
 
@@ -501,15 +504,11 @@ marl_status marl_ctx_autotune(marl_ctx* c, int32_t reps, float* best_us_out) {
             if (!plan_diffusion(&p, c->field[0], c->field[1], c->mask, c->g, tile, zc)) continue;
             std::swap(p, c->plan);
             // warm-up, then timed
-            for (int i = 0; i < 2; ++i) {
-                CK(launch_diffuse(c->plan, c->cur, c->field[c->cur], c->field[c->cur ^ 1], c->g, c->fk, 0,
-                                  &c->d_hdr->err, c->stream));
-            }
+            for (int i = 0; i < 2; ++i)
+                CK(launch_diffuse(c->plan, c->cur, c->g, c->fk, 0, nullptr, &c->d_hdr->err, c->stream));
             CK(cudaEventRecord(e0, c->stream));
-            for (int i = 0; i < reps; ++i) {
-                CK(launch_diffuse(c->plan, c->cur, c->field[c->cur], c->field[c->cur ^ 1], c->g, c->fk, 0,
-                                  &c->d_hdr->err, c->stream));
-            }
+            for (int i = 0; i < reps; ++i)
+                CK(launch_diffuse(c->plan, c->cur, c->g, c->fk, 0, nullptr, &c->d_hdr->err, c->stream));
             CK(cudaEventRecord(e1, c->stream));
             CK(cudaEventSynchronize(e1));
             float ms = 0;
@@ -629,7 +628,8 @@ marl_status marl_diffuse(marl_ctx* c, uint32_t substeps, int32_t fuse_sources) {
 
 marl_status marl_light_update(marl_ctx* c) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
-    CK(launch_light(c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
+    CK(launch_light(nullptr, c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
+    ++c->launches;
     return MARL_OK;
 }
 
@@ -650,9 +650,10 @@ marl_status marl_tick(marl_ctx* c, marl_change* changes, uint32_t cap, uint32_t*
     // crates/marl-sim/src/lib.rs:164-217: sources (fused into the first
     // substep), diffusion, light, the cell loop; then the ordered change list.
     const int span = span_begin(c);
-    marl_status st = enqueue_diffuse(c, c->sim.diffusion_substeps, true);
+    bool c4_ready = false;
+    marl_status st = enqueue_diffuse(c, c->sim.diffusion_substeps, true, true, &c4_ready);
     if (st) return st;
-    CK(launch_light(c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
+    CK(launch_light(c4_ready ? c->c4 : nullptr, c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
     ++c->launches;
     if ((st = enqueue_cell_phase(c))) return st;
     CK(launch_compact_events(c->t, c->n, c->d_block_counts, c->d_hdr, c->d_changes, c->t.cap, c->stream));
@@ -765,8 +766,7 @@ marl_status marl_diffuse_tick_with_cells(marl_ctx* c, float* field, const uint8_
     CK(cudaMemcpyAsync(c->d_occ_stage, occupancy, V, cudaMemcpyHostToDevice, c->stream));
     CK(launch_repack_mask(c->d_occ_stage, c->d_seam_mask, c->g, c->stream));
     for (uint32_t i = 0; i < c->sim.diffusion_substeps; ++i) {
-        CK(launch_diffuse(c->seam_plan, c->cur, c->field[c->cur], c->field[c->cur ^ 1], c->g, c->fk, 0,
-                          &c->d_hdr->err, c->stream));
+        CK(launch_diffuse(c->seam_plan, c->cur, c->g, c->fk, 0, nullptr, &c->d_hdr->err, c->stream));
         c->cur ^= 1;
     }
     CK(cudaMemcpyAsync(field, c->field[c->cur], V * 48, cudaMemcpyDeviceToHost, c->stream));
@@ -801,10 +801,9 @@ marl_status marl_diffuse_device(float* field_dev, float* scratch_dev, const uint
         cudaFreeAsync(err, s);
         return fail(MARL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     }
-    float* bufs[2] = {field_dev, scratch_dev};
-    int cur = 0;
+    int cur = 0;  // 0: field_dev holds the live state, 1: scratch_dev does
     for (uint32_t i = 0; i < substeps; ++i) {
-        CK(launch_diffuse(plan, cur, bufs[cur], bufs[cur ^ 1], g, fk, 0, err, s));
+        CK(launch_diffuse(plan, cur, g, fk, 0, nullptr, err, s));
         cur ^= 1;
     }
     if (cur != 0) CK(cudaMemcpyAsync(field_dev, scratch_dev, g.V() * 48, cudaMemcpyDeviceToDevice, s));

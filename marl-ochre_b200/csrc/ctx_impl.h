@@ -31,6 +31,7 @@ struct marl_ctx {
     uint8_t* mask = nullptr;   // [z][y][pitch] occupancy of the cell table
     int32_t* cmap = nullptr;   // [z][y][x] cell index or -1
     float* light = nullptr;    // [z][y][x]
+    float* c4 = nullptr;       // [z][y][x] species 4 after the last substep of a tick
     marl::CellTable t{};
     uint32_t n = 0;
     uint32_t epoch = 0;

@@ -5,7 +5,8 @@
 // aligned), exactly the reference's Field::data order
 // (crates/marl-field/src/field.rs:15-35), two ping-pong buffers; the occupancy
 // mask is u8 [z][y][pitch] with pitch = X rounded up to 16; light is f32
-// [z][y][x].
+// [z][y][x]; the last diffusion substep of a tick also writes species 4
+// compactly, f32 [z][y][x], for the light scan.
 //
 // Arithmetic is restated in the reference's operation order and this file is
 // compiled with -fmad=false, so diffusion and sources are bit-identical to the
@@ -57,34 +58,68 @@ __global__ void k_sources(float* __restrict__ f, Grid g, FieldConsts k) {
 // -------------------------------------------------------- diffusion ------
 // crates/marl-field/src/field.rs:107-203 (Field::diffusion_step_inner).
 //
-// 2.5D z-marching stencil.  A CTA owns a TX x TY column tile and a chunk of
-// `zc` planes.  Each xy plane of the tile plus a one-voxel halo (and the
-// matching occupancy rows) is brought into shared memory by one TMA load into
-// a 4-stage ring, three planes ahead of the plane being computed.  A thread
-// owns one (x, y) column: the z-1 and z+1 values of its own voxel live in
-// registers, the four xy neighbours come from the staged plane.
-template <int TX, int TY>
+// 2.5D z-marching stencil.  A CTA owns a 16 x TY column tile and a chunk of
+// `zc` planes.  Each xy plane of the tile plus a one-voxel halo is one TMA
+// load of a 3-D view of the field, {12*X floats, Y, Z}, whose box rows are
+// whole tile rows (18 voxels = 864 B); the matching occupancy rows come with
+// it on the same mbarrier.  Planes stream through a 4-stage ring three planes
+// ahead of the plane being computed.  A thread owns one (x, y) column: the
+// z-1 and z+1 values of its voxel live in registers, the four xy neighbours
+// come from the staged plane.  Results go to a double-buffered shared tile
+// that one TMA bulk-tensor store writes back per plane.
+constexpr int kDiffTX = 16;
+
+template <int TY>
 struct DiffTile {
+    static constexpr int TX = kDiffTX;
     static constexpr int PW = TX + 2, PH = TY + 2;
-    static constexpr int PLANE_BYTES = PW * PH * 12 * 4;
+    static constexpr int ROWF = PW * 12;  // floats per staged row: 216
+    static constexpr int PLANE_BYTES = PH * ROWF * 4;
     static constexpr int MW = TX + 32;  // mask box starts 16 columns left of the tile
     static constexpr int MASK_BYTES = MW * PH;
     static constexpr int MASK_REGION = (MASK_BYTES + 127) / 128 * 128;
-    static constexpr int STAGE_BYTES = MASK_REGION + (PLANE_BYTES + 127) / 128 * 128;
+    static constexpr int PLANE_REGION = (PLANE_BYTES + 127) / 128 * 128;
+    static constexpr int STAGE_BYTES = MASK_REGION + PLANE_REGION;
     static constexpr int STAGES = 4;
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + STAGES * 8;
-    static_assert(TX % 16 == 0, "mask TMA box needs 16-byte aligned x start");
-    static_assert(PW <= 256 && PH <= 256 && MW <= 256, "TMA box dims are limited to 256");
+    static constexpr int OUT_BYTES = TY * TX * 48;
+    static constexpr int OUT_BUFS = 2;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + OUT_BUFS * OUT_BYTES + STAGES * 8;
+    static_assert(ROWF <= 256 && TX * 12 <= 256 && PH <= 256 && MW <= 256, "TMA box dims are limited to 256");
+    static_assert(OUT_BYTES % 128 == 0, "output staging alignment");
 };
 
-template <int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) k_diffuse(const __grid_constant__ CUtensorMap tm_field,
-                                                    const __grid_constant__ CUtensorMap tm_mask,
-                                                    float* __restrict__ dst, Grid g, int zc, FieldConsts k,
-                                                    int apply_sources, uint32_t* __restrict__ err) {
-    using T = DiffTile<TX, TY>;
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void load12(float* d, const float* s) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const float4 a = reinterpret_cast<const float4*>(s)[q];
+        d[4 * q] = a.x, d[4 * q + 1] = a.y, d[4 * q + 2] = a.z, d[4 * q + 3] = a.w;
+    }
+}
+
+template <int TY>
+__global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__ CUtensorMap tm_src,
+                                                        const __grid_constant__ CUtensorMap tm_dst,
+                                                        const __grid_constant__ CUtensorMap tm_mask, Grid g, int zc,
+                                                        FieldConsts k, int apply_sources, float* __restrict__ c4_out,
+                                                        uint32_t* __restrict__ err) {
+    using T = DiffTile<TY>;
+    constexpr int TX = T::TX;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T::STAGES * T::STAGE_BYTES);
+    float* outbuf = reinterpret_cast<float*>(smem + T::STAGES * T::STAGE_BYTES);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T::STAGES * T::STAGE_BYTES + T::OUT_BUFS * T::OUT_BYTES);
     __shared__ int s_abort;
 
     const int tid = threadIdx.x;
@@ -105,7 +140,7 @@ __global__ void __launch_bounds__(TX* TY) k_diffuse(const __grid_constant__ CUte
         // Planes outside the grid are never read (walls use the centre
         // value), so they are loaded from a clamped in-grid z.
         const int zz = min(max(z0 - 1 + p, 0), g.Z - 1);
-        tma_load_4d(plane_of(p), &tm_field, 0, x0 - 1, y0 - 1, zz, bar);
+        tma_load_3d(plane_of(p), &tm_src, (x0 - 1) * 12, y0 - 1, zz, bar);
         tma_load_3d((void*)mask_of(p), &tm_mask, x0 - 16, y0 - 1, zz, bar);
     };
     auto transform = [&](int p) {  // boundary sources applied to a staged plane
@@ -147,23 +182,22 @@ __global__ void __launch_bounds__(TX* TY) k_diffuse(const __grid_constant__ CUte
     float below[12], cur[12], above[12];
     bool mb = false, mc = false, ma = false;
     if (!s_abort) {
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const float4 a = reinterpret_cast<const float4*>(plane_of(0) + ci)[q];
-            const float4 b = reinterpret_cast<const float4*>(plane_of(1) + ci)[q];
-            below[4 * q] = a.x, below[4 * q + 1] = a.y, below[4 * q + 2] = a.z, below[4 * q + 3] = a.w;
-            cur[4 * q] = b.x, cur[4 * q + 1] = b.y, cur[4 * q + 2] = b.z, cur[4 * q + 3] = b.w;
-        }
+        load12(below, plane_of(0) + ci);
+        load12(cur, plane_of(1) + ci);
         mb = mask_of(0)[mi] != 0;
         mc = mask_of(1)[mi] != 0;
     }
     __syncthreads();
 
     for (int p = 1; p <= nplanes - 2 && !s_abort; ++p) {
-        if (tid == 0 && p + 3 < nplanes) {
-            fence_proxy_async_smem();
-            issue(p + 3);
-            issued = p + 4;
+        if (tid == 0) {
+            if (p + 3 < nplanes) {
+                fence_proxy_async_smem();
+                issue(p + 3);
+                issued = p + 4;
+            }
+            // the output buffer used now was last handed to a store two planes ago
+            bulk_wait_read<1>();
         }
         if (!mbar_wait_bounded(&bars[(p + 1) % T::STAGES], ((p + 1) / T::STAGES) & 1)) {
             atomicOr(err, kErrTimeoutMbar);
@@ -174,63 +208,54 @@ __global__ void __launch_bounds__(TX* TY) k_diffuse(const __grid_constant__ CUte
         __syncthreads();
         if (s_abort) break;
 
-        const float* Pn = plane_of(p + 1);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const float4 a = reinterpret_cast<const float4*>(Pn + ci)[q];
-            above[4 * q] = a.x, above[4 * q + 1] = a.y, above[4 * q + 2] = a.z, above[4 * q + 3] = a.w;
-        }
+        load12(above, plane_of(p + 1) + ci);
         ma = mask_of(p + 1)[mi] != 0;
 
         const int z = z0 - 1 + p;
-        if (active) {
-            float out[12];
-            if (mc) {  // occupied: copied unchanged (field.rs:130-136)
+        float out[12];
+        if (mc) {  // occupied: copied unchanged (field.rs:130-136)
 #pragma unroll
-                for (int s = 0; s < 12; ++s) out[s] = cur[s];
-            } else {
-                const float* P = plane_of(p);
-                const uint8_t* M = mask_of(p);
-                const float structural = cur[7];
-                const float niche = 1.0f - k.alpha_eps * structural / (k.k_eps + structural);
-                const bool wxm = x == 0 || M[mi - 1];
-                const bool wxp = x >= g.X - 1 || M[mi + 1];
-                const bool wym = y == 0 || M[mi - T::MW];
-                const bool wyp = y >= g.Y - 1 || M[mi + T::MW];
-                const bool wzm = z == 0 || mb;
-                const bool wzp = z >= g.Z - 1 || ma;
-                float nxm[12], nxp[12], nym[12], nyp[12];
+            for (int s = 0; s < 12; ++s) out[s] = cur[s];
+        } else {
+            const float* P = plane_of(p);
+            const uint8_t* M = mask_of(p);
+            const float structural = cur[7];
+            const float niche = 1.0f - k.alpha_eps * structural / (k.k_eps + structural);
+            // A wall or occupied neighbour reads as the centre value: point
+            // its load at the centre voxel.
+            const float* pxm = (x == 0 || M[mi - 1]) ? P + ci : P + ci - 12;
+            const float* pxp = (x >= g.X - 1 || M[mi + 1]) ? P + ci : P + ci + 12;
+            const float* pym = (y == 0 || M[mi - T::MW]) ? P + ci : P + ci - T::ROWF;
+            const float* pyp = (y >= g.Y - 1 || M[mi + T::MW]) ? P + ci : P + ci + T::ROWF;
+            const bool wzm = z == 0 || mb;
+            const bool wzp = z >= g.Z - 1 || ma;
+            float nxm[12], nxp[12], nym[12], nyp[12];
+            load12(nxm, pxm);
+            load12(nxp, pxp);
+            load12(nym, pym);
+            load12(nyp, pyp);
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    const float4 a = reinterpret_cast<const float4*>(P + ci - 12)[q];
-                    const float4 b = reinterpret_cast<const float4*>(P + ci + 12)[q];
-                    const float4 c = reinterpret_cast<const float4*>(P + ci - T::PW * 12)[q];
-                    const float4 d = reinterpret_cast<const float4*>(P + ci + T::PW * 12)[q];
-                    nxm[4 * q] = a.x, nxm[4 * q + 1] = a.y, nxm[4 * q + 2] = a.z, nxm[4 * q + 3] = a.w;
-                    nxp[4 * q] = b.x, nxp[4 * q + 1] = b.y, nxp[4 * q + 2] = b.z, nxp[4 * q + 3] = b.w;
-                    nym[4 * q] = c.x, nym[4 * q + 1] = c.y, nym[4 * q + 2] = c.z, nym[4 * q + 3] = c.w;
-                    nyp[4 * q] = d.x, nyp[4 * q + 1] = d.y, nyp[4 * q + 2] = d.z, nyp[4 * q + 3] = d.w;
-                }
-#pragma unroll
-                for (int s = 0; s < 12; ++s) {  // field.rs:152-195
-                    const float c = cur[s];
-                    const float d = k.d_voxel[s] * niche;
-                    const float xm = wxm ? c : nxm[s];
-                    const float xp = wxp ? c : nxp[s];
-                    const float ym = wym ? c : nym[s];
-                    const float yp = wyp ? c : nyp[s];
-                    const float zm = wzm ? c : below[s];
-                    const float zp = wzp ? c : above[s];
-                    const float lap = xm + xp + ym + yp + zm + zp - 6.0f * c;
-                    const float decay = k.lambda_decay[s] * c;
-                    const float nc = c + k.dt_sub * (d * lap - decay);
-                    out[s] = fmaxf(nc, 0.0f);
-                }
+            for (int s = 0; s < 12; ++s) {  // field.rs:152-195
+                const float c = cur[s];
+                const float d = k.d_voxel[s] * niche;
+                const float zm = wzm ? c : below[s];
+                const float zp = wzp ? c : above[s];
+                const float lap = nxm[s] + nxp[s] + nym[s] + nyp[s] + zm + zp - 6.0f * c;
+                const float decay = k.lambda_decay[s] * c;
+                const float nc = c + k.dt_sub * (d * lap - decay);
+                out[s] = fmaxf(nc, 0.0f);
             }
-            float4* o = reinterpret_cast<float4*>(dst + (((size_t)z * g.Y + y) * g.X + x) * 12);
-            o[0] = make_float4(out[0], out[1], out[2], out[3]);
-            o[1] = make_float4(out[4], out[5], out[6], out[7]);
-            o[2] = make_float4(out[8], out[9], out[10], out[11]);
+        }
+        float* ob = outbuf + (p & 1) * (T::OUT_BYTES / 4) + (ty * TX + tx) * 12;
+        reinterpret_cast<float4*>(ob)[0] = make_float4(out[0], out[1], out[2], out[3]);
+        reinterpret_cast<float4*>(ob)[1] = make_float4(out[4], out[5], out[6], out[7]);
+        reinterpret_cast<float4*>(ob)[2] = make_float4(out[8], out[9], out[10], out[11]);
+        if (c4_out && active) c4_out[((size_t)z * g.Y + y) * g.X + x] = out[4];
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tma_store_3d(&tm_dst, outbuf + (p & 1) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
+            bulk_commit();
         }
 #pragma unroll
         for (int s = 0; s < 12; ++s) {
@@ -239,59 +264,61 @@ __global__ void __launch_bounds__(TX* TY) k_diffuse(const __grid_constant__ CUte
         }
         mb = mc;
         mc = ma;
-        __syncthreads();
     }
 
-    // Drain: after an abort, wait (bounded) for loads still in flight so no
-    // copy lands in shared memory after the CTA exits.
-    if (s_abort && tid == 0) {
-        for (int q = waited; q < issued; ++q) mbar_wait_bounded(&bars[q % T::STAGES], (q / T::STAGES) & 1);
+    if (tid == 0) {
+        bulk_wait_all();
+        // After an abort, wait (bounded) for loads still in flight so no copy
+        // lands in shared memory after the CTA exits.
+        if (s_abort)
+            for (int q = waited; q < issued; ++q) mbar_wait_bounded(&bars[q % T::STAGES], (q / T::STAGES) & 1);
     }
 }
 
 // ------------------------------------------------------------ light ------
-// crates/marl-field/src/light.rs:29-59.  One thread per (x, y) column, z in
-// order: the running intensity is an exclusive product with a floor to zero,
-// which is not associative, so it is kept sequential per column to stay
-// identical to the reference.  exp is evaluated in double and rounded to
-// float (the reference calls glibc expf, which is within 0.502 ulp).
-__global__ void k_light(const float* __restrict__ field, const uint8_t* __restrict__ mask, float* __restrict__ light,
-                        Grid g, FieldConsts k) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= g.X * g.Y) return;
-    const int x = col % g.X, y = col / g.X;
+// crates/marl-field/src/light.rs:29-59.  The running intensity of a column is
+// an exclusive product with a floor to zero; the floor makes it
+// non-associative, so each column is multiplied strictly in z order.  A block
+// covers 32 columns of one y row: all 256 threads first evaluate the
+// attenuation factors of a 64-plane segment in parallel (exp in double,
+// rounded to float: the reference calls glibc expf, within 0.502 ulp), then
+// one warp runs the 32 sequential column products through that segment.
+constexpr int kLightCols = 32;
+constexpr int kLightSeg = 64;
+
+__global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, const float* __restrict__ field,
+                                               const uint8_t* __restrict__ mask, float* __restrict__ light, Grid g,
+                                               FieldConsts k) {
+    __shared__ float fac[kLightSeg][kLightCols];
+    __shared__ uint8_t occ[kLightSeg][kLightCols];
+    const int x0 = blockIdx.x * kLightCols, y = blockIdx.y;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int pitch = mask_pitch(g.X);
-    const size_t plane = (size_t)g.X * g.Y;
-    float inten = k.surface_intensity;
     const float neg_chem = -k.chemical_absorption;
-    constexpr int U = 8;
-    int z = 0;
-    for (; z + U <= g.Z; z += U) {
-        float a[U];
-        uint8_t m[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const size_t v = (size_t)(z + u) * plane + col;
-            a[u] = __ldg(field + v * 12 + 4);
-            m[u] = __ldg(mask + ((size_t)(z + u) * g.Y + y) * pitch + x);
+    float inten = k.surface_intensity;
+    for (int zs = 0; zs < g.Z; zs += kLightSeg) {
+        const int nz = min(kLightSeg, g.Z - zs);
+        for (int i = tid; i < nz * kLightCols; i += 256) {
+            const int zz = i / kLightCols, xi = i % kLightCols, xg = x0 + xi;
+            if (xg < g.X) {
+                const size_t v = ((size_t)(zs + zz) * g.Y + y) * g.X + xg;
+                const float a = c4 ? c4[v] : field[v * 12 + 4];
+                fac[zz][xi] = (float)exp((double)(neg_chem * a));
+                occ[zz][xi] = mask[((size_t)(zs + zz) * g.Y + y) * pitch + xg];
+            }
         }
-        float e[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) e[u] = (float)exp((double)(neg_chem * a[u]));
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            light[(size_t)(z + u) * plane + col] = inten;
-            if (m[u]) inten *= k.cell_factor;
-            inten *= e[u];
-            if (inten < k.light_floor) inten = 0.0f;
+        __syncthreads();
+        if (tid < 32 && x0 + lane < g.X) {
+            float* out = light + ((size_t)zs * g.Y + y) * g.X + x0 + lane;
+            const size_t plane = (size_t)g.X * g.Y;
+            for (int zz = 0; zz < nz; ++zz) {
+                out[zz * plane] = inten;
+                if (occ[zz][lane]) inten *= k.cell_factor;
+                inten *= fac[zz][lane];
+                if (inten < k.light_floor) inten = 0.0f;
+            }
         }
-    }
-    for (; z < g.Z; ++z) {
-        const size_t v = (size_t)z * plane + col;
-        light[v] = inten;
-        if (mask[((size_t)z * g.Y + y) * pitch + x]) inten *= k.cell_factor;
-        inten *= (float)exp((double)(neg_chem * field[v * 12 + 4]));
-        if (inten < k.light_floor) inten = 0.0f;
+        __syncthreads();
     }
 }
 
@@ -366,41 +393,41 @@ __global__ void k_unpack_mask(const uint8_t* __restrict__ mask, uint8_t* __restr
 
 // ======================================================== launchers ======
 
-template <int TX, int TY>
-static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, const CUtensorMap* tm_field, const float* src,
-                                    float* dst, const Grid& g, const FieldConsts& k, int apply_sources,
-                                    uint32_t* err, cudaStream_t s) {
-    using T = DiffTile<TX, TY>;
-    (void)src;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_diffuse<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             T::SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    dim3 grid((g.X + TX - 1) / TX, (g.Y + TY - 1) / TY, (g.Z + plan.zc - 1) / plan.zc);
-    k_diffuse<TX, TY><<<grid, TX * TY, T::SMEM_BYTES, s>>>(*tm_field, plan.tm_mask, dst, g, plan.zc, k,
-                                                            apply_sources, err);
-    return cudaGetLastError();
-}
+static const int kTileTY[] = {8, 16, 4, 32};
 
 int diffusion_tile_count() { return 4; }
 
 void diffusion_tile_shape(int tile, int* tx, int* ty) {
-    static const int shapes[4][2] = {{32, 8}, {32, 4}, {64, 4}, {16, 16}};
-    *tx = shapes[tile][0];
-    *ty = shapes[tile][1];
+    *tx = kDiffTX;
+    *ty = kTileTY[tile];
 }
 
-cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const float* src, float* dst, const Grid& g,
-                           const FieldConsts& k, int apply_sources, uint32_t* err, cudaStream_t s) {
-    const CUtensorMap* tm = which_src == 0 ? &plan.tm_field[0] : &plan.tm_field[1];
+template <int TY>
+static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
+                                    int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
+    using T = DiffTile<TY>;
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e = cudaFuncSetAttribute(k_diffuse<TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             T::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    dim3 grid((g.X + kDiffTX - 1) / kDiffTX, (g.Y + TY - 1) / TY, (g.Z + plan.zc - 1) / plan.zc);
+    k_diffuse<TY><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(plan.tm_load[which_src], plan.tm_store[which_src ^ 1],
+                                                            plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
+                           int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
     switch (plan.tile) {
-        case 0: return launch_diffuse_t<32, 8>(plan, tm, src, dst, g, k, apply_sources, err, s);
-        case 1: return launch_diffuse_t<32, 4>(plan, tm, src, dst, g, k, apply_sources, err, s);
-        case 2: return launch_diffuse_t<64, 4>(plan, tm, src, dst, g, k, apply_sources, err, s);
-        default: return launch_diffuse_t<16, 16>(plan, tm, src, dst, g, k, apply_sources, err, s);
+        case 0: return launch_diffuse_t<8>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 1: return launch_diffuse_t<16>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 2: return launch_diffuse_t<4>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        default: return launch_diffuse_t<32>(plan, which_src, g, k, apply_sources, c4_out, err, s);
     }
 }
 
@@ -410,10 +437,10 @@ cudaError_t launch_sources(float* f, const Grid& g, const FieldConsts& k, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_light(const float* f, const uint8_t* mask, float* light, const Grid& g, const FieldConsts& k,
-                         cudaStream_t s) {
-    const int n = g.X * g.Y;
-    k_light<<<(n + 127) / 128, 128, 0, s>>>(f, mask, light, g, k);
+cudaError_t launch_light(const float* c4, const float* f, const uint8_t* mask, float* light, const Grid& g,
+                         const FieldConsts& k, cudaStream_t s) {
+    dim3 grid((g.X + kLightCols - 1) / kLightCols, g.Y);
+    k_light<<<grid, 256, 0, s>>>(c4, f, mask, light, g, k);
     return cudaGetLastError();
 }
 
@@ -449,14 +476,16 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-bool encode_field_map(CUtensorMap* m, const float* base, const Grid& g, int tx, int ty) {
+// 3-D view {12*X floats, Y, Z} of a field buffer with a box of `box_voxels`
+// voxels by `box_rows` rows by one plane.
+bool encode_field_map(CUtensorMap* m, const float* base, const Grid& g, int box_voxels, int box_rows) {
     auto fn = encode_fn();
     if (!fn) return false;
-    const cuuint64_t dims[4] = {12, (cuuint64_t)g.X, (cuuint64_t)g.Y, (cuuint64_t)g.Z};
-    const cuuint64_t strides[3] = {48, (cuuint64_t)g.X * 48, (cuuint64_t)g.X * g.Y * 48};
-    const cuuint32_t box[4] = {12, (cuuint32_t)(tx + 2), (cuuint32_t)(ty + 2), 1};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void*)base, dims, strides, box, estr,
+    const cuuint64_t dims[3] = {(cuuint64_t)g.X * 12, (cuuint64_t)g.Y, (cuuint64_t)g.Z};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.X * 48, (cuuint64_t)g.X * g.Y * 48};
+    const cuuint32_t box[3] = {(cuuint32_t)(box_voxels * 12), (cuuint32_t)box_rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -480,8 +509,12 @@ bool plan_diffusion(DiffusionPlan* plan, const float* a, const float* b, const u
     diffusion_tile_shape(tile, &tx, &ty);
     plan->tile = tile;
     plan->zc = zc > 0 ? zc : 16;
-    return encode_field_map(&plan->tm_field[0], a, g, tx, ty) && encode_field_map(&plan->tm_field[1], b, g, tx, ty) &&
-           encode_mask_map(&plan->tm_mask, mask, g, tx, ty);
+    const float* bufs[2] = {a, b};
+    for (int i = 0; i < 2; ++i) {
+        if (!encode_field_map(&plan->tm_load[i], bufs[i], g, tx + 2, ty + 2)) return false;
+        if (!encode_field_map(&plan->tm_store[i], bufs[i], g, tx, ty)) return false;
+    }
+    return encode_mask_map(&plan->tm_mask, mask, g, tx, ty);
 }
 
 }  // namespace marl

@@ -14,7 +14,8 @@ namespace marl {
 // Tensor maps and tile choice for the diffusion kernel over one pair of
 // ping-pong buffers and one occupancy mask.
 struct DiffusionPlan {
-    CUtensorMap tm_field[2];  // source = buffer 0 / buffer 1
+    CUtensorMap tm_load[2];   // halo'd plane loads from buffer 0 / buffer 1
+    CUtensorMap tm_store[2];  // tile stores into buffer 0 / buffer 1
     CUtensorMap tm_mask;
     int tile = 0;  // index into the tile-shape table
     int zc = 16;   // z-chunk per CTA
@@ -22,16 +23,19 @@ struct DiffusionPlan {
 
 int diffusion_tile_count();
 void diffusion_tile_shape(int tile, int* tx, int* ty);
-bool encode_field_map(CUtensorMap* m, const float* base, const Grid& g, int tx, int ty);
+bool encode_field_map(CUtensorMap* m, const float* base, const Grid& g, int box_voxels, int box_rows);
 bool encode_mask_map(CUtensorMap* m, const uint8_t* base, const Grid& g, int tx, int ty);
 bool plan_diffusion(DiffusionPlan* plan, const float* a, const float* b, const uint8_t* mask, const Grid& g,
                     int tile, int zc);
 
 cudaError_t launch_sources(float* f, const Grid& g, const FieldConsts& k, cudaStream_t s);
-cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const float* src, float* dst, const Grid& g,
-                           const FieldConsts& k, int apply_sources, uint32_t* err, cudaStream_t s);
-cudaError_t launch_light(const float* f, const uint8_t* mask, float* light, const Grid& g, const FieldConsts& k,
-                         cudaStream_t s);
+// One substep from buffer `which_src` into the other buffer of the plan.
+// c4_out (nullable) receives species 4 of the result, [z][y][x].
+cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
+                           int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s);
+// c4 (nullable): compact species 4 of `f`; when null species 4 is read from f.
+cudaError_t launch_light(const float* c4, const float* f, const uint8_t* mask, float* light, const Grid& g,
+                         const FieldConsts& k, cudaStream_t s);
 cudaError_t launch_mass(const float* f, const Grid& g, double* partial, double* out, cudaStream_t s);
 size_t mass_partial_doubles();
 cudaError_t launch_repack_mask(const uint8_t* occ, uint8_t* mask, const Grid& g, cudaStream_t s);

@@ -171,7 +171,9 @@ def light_case(marl, oracle_mod, dims, seed, absorber_hi=3.0, occ_frac=0.1):
 def test_light_matches_oracle(marl, oracle_mod, dims):
     gpu, cpu, cpu64 = light_case(marl, oracle_mod, dims, 3)
     np.testing.assert_allclose(gpu, cpu, rtol=LIGHT_RTOL, atol=LIGHT_ATOL)
-    assert np.mean(gpu == cpu) > 0.99  # exp differs from glibc expf by <= 1 ulp on a few voxels
+    # exp differs from glibc expf by <= 1 ulp on a few voxels; a difference
+    # then carries down the rest of its column
+    assert np.mean(gpu == cpu) > 0.95
     # error against the FP64 oracle is no worse than the FP32 oracle's own
     err_gpu = np.abs(gpu - cpu64).max()
     err_cpu = np.abs(cpu - cpu64).max()
