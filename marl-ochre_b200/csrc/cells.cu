@@ -97,19 +97,19 @@ __device__ __forceinline__ float rclamp(float v, float lo, float hi) {  // Rust 
     return v;
 }
 
-__device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uint32_t nb) {
+// Everything a cell's update needs that no other cell of this tick writes:
+// staged before the cell waits on its dependencies.
+struct CellPre {
+    uint32_t nb, pos, state;
+    float light;
+    int32_t dep[6];
+};
+
+__device__ __forceinline__ void stage_cell(const CellLaunch& a, CellScratch& S, uint32_t j, CellPre& pre) {
     const int tid = threadIdx.x;
     const CellTable& t = a.t;
     const size_t cap = t.cap;
-    const Grid g = a.g;
-    const uint32_t P = t.pos[j];
-    const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
-    const size_t vox = ((size_t)z * g.Y + y) * g.X + x;
-    const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
-                              -(long long)g.X * g.Y};
-    const int n = __popc(nb);
-
-    // Stage the ruleset and internal state (asynchronous copies).
+    // Ruleset and internal state: asynchronous copies into shared memory.
 #pragma unroll
     for (int r = 0; r < MARL_R_MAX; ++r) cp_async16(&S.rx[r][tid], &t.rx[r * cap + j]);
 #pragma unroll
@@ -121,8 +121,29 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
     cp_async16(&S.fate[tid], &t.fate[j]);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) cp_async4(&S.x[k][tid], &t.internal[k * cap + j]);
-    const uint32_t st0 = t.state[j];
-    const float light = a.light[vox];
+    pre.nb = t.nb[j];
+    pre.pos = t.pos[j];
+    pre.state = t.state[j];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) pre.dep[f] = ((pre.nb >> f) & 1u) ? t.dep[(size_t)f * cap + j] : -1;
+    const Grid g = a.g;
+    pre.light = a.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
+}
+
+// Gather -> tick -> scatter of cell j, after all its dependencies are done.
+__device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, const CellPre& pre) {
+    const int tid = threadIdx.x;
+    const CellTable& t = a.t;
+    const Grid g = a.g;
+    const uint32_t nb = pre.nb;
+    const uint32_t P = pre.pos;
+    const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
+    const size_t vox = ((size_t)z * g.Y + y) * g.X + x;
+    const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
+                              -(long long)g.X * g.Y};
+    const int n = __popc(nb);
+    const uint32_t st0 = pre.state;
+    const float light = pre.light;
 
     // Gather: mean of the empty face neighbours (spatial.rs:56-77).
 #pragma unroll
@@ -258,7 +279,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, uin
     t.state[j] = (st & 0xFF000000u) | (quiescent << 16) | prep;
     t.events[j] = event;
 #pragma unroll
-    for (int k = 0; k < MARL_M_INT; ++k) t.internal[k * cap + j] = S.x[k][tid];
+    for (int k = 0; k < MARL_M_INT; ++k) t.internal[(size_t)k * t.cap + j] = S.x[k][tid];
 
     // Scatter: split deltas over the same neighbours, clamp after each add
     // (spatial.rs:87-110, field.rs:57-62).
@@ -297,19 +318,18 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(CellLaunch a) {
         if (base >= a.n) break;
         const uint32_t j = base + lane;
         bool pending = j < a.n;
-        const uint32_t nb = pending ? t.nb[j] : 0u;
+        CellPre pre;
+        if (pending) stage_cell(a, S, j, pre);
         uint32_t spins = 0;
         while (__any_sync(FULL, pending)) {
             if (pending) {
                 bool ready = true;
-                for (int f = 0; f < 6; ++f) {
-                    if (!((nb >> f) & 1u)) continue;
-                    const int32_t d = t.dep[(size_t)f * t.cap + j];
-                    if (d >= 0 && ld_acquire_u32(&t.done[d]) != a.epoch) ready = false;
-                }
+#pragma unroll
+                for (int f = 0; f < 6; ++f)
+                    if (pre.dep[f] >= 0 && ld_acquire_u32(&t.done[pre.dep[f]]) != a.epoch) ready = false;
                 if (ready) {
-                    update_cell(a, S, j, nb);
-                    __threadfence();
+                    update_cell(a, S, j, pre);
+                    // release: this cell's field writes are visible before its done flag
                     st_release_u32(&t.done[j], a.epoch);
                     pending = false;
                 }
@@ -318,6 +338,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(CellLaunch a) {
                 if (++spins > kFlagSpinLimit) {
                     if (pending) {
                         atomicOr(a.err, kErrTimeoutDeps);
+                        cp_async_wait_all();  // drain this lane's staging copies
                         t.events[j] = MARL_EVENT_NONE;
                         st_release_u32(&t.done[j], a.epoch);
                         pending = false;

@@ -56,20 +56,17 @@ __global__ void k_sources(float* __restrict__ f, Grid g, FieldConsts k) {
 }
 
 // -------------------------------------------------------- diffusion ------
-// crates/marl-field/src/field.rs:107-203 (Field::diffusion_step_inner).
-//
-// 2.5D z-marching stencil.  A CTA owns a 16 x TY column tile and a chunk of
-// `zc` planes.  Each xy plane of the tile plus a one-voxel halo is one TMA
-// load of a 3-D view of the field, {12*X floats, Y, Z}, whose box rows are
-// whole tile rows (18 voxels = 864 B); the matching occupancy rows come with
-// it on the same mbarrier.  Planes stream through a 4-stage ring three planes
-// ahead of the plane being computed.  A thread owns one (x, y) column: the
-// z-1 and z+1 values of its voxel live in registers, the four xy neighbours
-// come from the staged plane.  Results go to a double-buffered shared tile
-// that one TMA bulk-tensor store writes back per plane.
+// Stencil arithmetic: 1 (default) = packed FP32x2 adds with scalar
+// multiplies, 0 = all scalar.  Both are bit-identical to the reference.  The
+// multiplies stay scalar because ptxas may contract a packed multiply that
+// feeds a packed add into one fused FFMA2 (observed: 45% of results off by an
+// ulp), while a scalar __fmul_rn feeding a packed add is never fused.
+#ifndef MARL_STENCIL_MODE
+#define MARL_STENCIL_MODE 1
+#endif
 constexpr int kDiffTX = 16;
 
-template <int TY>
+template <int TY, int STAGES>
 struct DiffTile {
     static constexpr int TX = kDiffTX;
     static constexpr int PW = TX + 2, PH = TY + 2;
@@ -80,12 +77,12 @@ struct DiffTile {
     static constexpr int MASK_REGION = (MASK_BYTES + 127) / 128 * 128;
     static constexpr int PLANE_REGION = (PLANE_BYTES + 127) / 128 * 128;
     static constexpr int STAGE_BYTES = MASK_REGION + PLANE_REGION;
-    static constexpr int STAGES = 4;
     static constexpr int OUT_BYTES = TY * TX * 48;
-    static constexpr int OUT_BUFS = 2;
+    static constexpr int OUT_BUFS = 3;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + OUT_BUFS * OUT_BYTES + STAGES * 8;
     static_assert(ROWF <= 256 && TX * 12 <= 256 && PH <= 256 && MW <= 256, "TMA box dims are limited to 256");
     static_assert(OUT_BYTES % 128 == 0, "output staging alignment");
+    static_assert(STAGES == 3 || STAGES == 4, "3 or 4 plane stages");
 };
 
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1, int c2) {
@@ -101,41 +98,140 @@ __device__ __forceinline__ void bulk_wait_read() {
 }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-__device__ __forceinline__ void load12(float* d, const float* s) {
+// Twelve species as six float2 pairs (species 2q, 2q+1).
+struct Vox {
+    float2 v[6];
+};
+__device__ __forceinline__ void load_vox(Vox& d, const float* s) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
         const float4 a = reinterpret_cast<const float4*>(s)[q];
-        d[4 * q] = a.x, d[4 * q + 1] = a.y, d[4 * q + 2] = a.z, d[4 * q + 3] = a.w;
+        d.v[2 * q] = make_float2(a.x, a.y);
+        d.v[2 * q + 1] = make_float2(a.z, a.w);
     }
 }
 
-template <int TY>
+// Packed FP32x2 add: each lane is the IEEE round-to-nearest single-precision
+// sum (checked lane by lane against add.rn.f32 on the device).
+__device__ __forceinline__ uint64_t pk2(float2 v) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(uint64_t r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(r);
+}
+
+// Per-voxel update: the reference expression
+//   c + dt*(d*(xm+xp+ym+yp+zm+zp - 6c) - lambda*c), then max(., 0)
+// evaluated in the same order (a - b is a + (-b) exactly).
+__device__ __forceinline__ void stencil(float out[12], const Vox& c, const Vox& xm, const Vox& xp, const Vox& ym,
+                                        const Vox& yp, const Vox& below, const Vox& above, bool wzm, bool wzp,
+                                        const FieldConsts& k) {
+    const float structural = c.v[3].y;  // species 7
+    const float niche = 1.0f - k.alpha_eps * structural / (k.k_eps + structural);
+#if MARL_STENCIL_MODE == 0
+    // Scalar IEEE operations (no contraction possible).
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const float2 cc = c.v[q];
+        const float2 zm = wzm ? cc : below.v[q];
+        const float2 zp = wzp ? cc : above.v[q];
+        float r[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float cv = h ? cc.y : cc.x;
+            const float d = __fmul_rn(k.d_voxel[2 * q + h], niche);
+            float lap = __fadd_rn(h ? xm.v[q].y : xm.v[q].x, h ? xp.v[q].y : xp.v[q].x);
+            lap = __fadd_rn(lap, h ? ym.v[q].y : ym.v[q].x);
+            lap = __fadd_rn(lap, h ? yp.v[q].y : yp.v[q].x);
+            lap = __fadd_rn(lap, h ? zm.y : zm.x);
+            lap = __fadd_rn(lap, h ? zp.y : zp.x);
+            lap = __fsub_rn(lap, __fmul_rn(6.0f, cv));
+            const float t = __fsub_rn(__fmul_rn(d, lap), __fmul_rn(k.lambda_decay[2 * q + h], cv));
+            r[h] = fmaxf(__fadd_rn(cv, __fmul_rn(k.dt_sub, t)), 0.0f);
+        }
+        out[2 * q] = r[0];
+        out[2 * q + 1] = r[1];
+    }
+#else
+    // Packed adds, scalar multiplies.
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const float2 cc = c.v[q];
+        const float2 zm = wzm ? cc : below.v[q];
+        const float2 zp = wzp ? cc : above.v[q];
+        const float2 d = make_float2(__fmul_rn(k.d_voxel[2 * q], niche), __fmul_rn(k.d_voxel[2 * q + 1], niche));
+        float2 lap = add2_rn(xm.v[q], xp.v[q]);
+        lap = add2_rn(lap, ym.v[q]);
+        lap = add2_rn(lap, yp.v[q]);
+        lap = add2_rn(lap, zm);
+        lap = add2_rn(lap, zp);
+        lap = add2_rn(lap, make_float2(__fmul_rn(-6.0f, cc.x), __fmul_rn(-6.0f, cc.y)));
+        const float2 ndecay = make_float2(__fmul_rn(-k.lambda_decay[2 * q], cc.x),
+                                          __fmul_rn(-k.lambda_decay[2 * q + 1], cc.y));
+        const float2 t = add2_rn(make_float2(__fmul_rn(d.x, lap.x), __fmul_rn(d.y, lap.y)), ndecay);
+        const float2 nc = add2_rn(cc, make_float2(__fmul_rn(k.dt_sub, t.x), __fmul_rn(k.dt_sub, t.y)));
+        out[2 * q] = fmaxf(nc.x, 0.0f);
+        out[2 * q + 1] = fmaxf(nc.y, 0.0f);
+    }
+#endif
+
+}
+
+// crates/marl-field/src/field.rs:107-203 (Field::diffusion_step_inner).
+//
+// 2.5D z-marching stencil.  A CTA owns a 16 x TY column tile and a chunk of
+// `zc` planes.  Each xy plane of the tile plus a one-voxel halo is one TMA
+// load of a 3-D view of the field, {12*X floats, Y, Z}, whose box rows are
+// whole tile rows (18 voxels = 864 B); the matching occupancy rows come with
+// it on the same mbarrier.  Planes stream through a ring of STAGES stages,
+// STAGES-1 planes ahead of the plane being computed.  A thread owns one
+// (x, y) column: the below / centre / above values of its voxel rotate
+// through three register sets (the loop is unrolled by three, no copies),
+// the four xy neighbours come from the staged plane, and the wall flags of
+// the next plane are read one plane early so the neighbour loads never wait
+// on them.  Results go to a triple-buffered shared tile; one TMA bulk-tensor
+// store per plane writes it back.  One barrier per plane.
+template <int TY, int STAGES>
 __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__ CUtensorMap tm_src,
                                                         const __grid_constant__ CUtensorMap tm_dst,
                                                         const __grid_constant__ CUtensorMap tm_mask, Grid g, int zc,
                                                         FieldConsts k, int apply_sources, float* __restrict__ c4_out,
                                                         uint32_t* __restrict__ err) {
-    using T = DiffTile<TY>;
+    using T = DiffTile<TY, STAGES>;
     constexpr int TX = T::TX;
     extern __shared__ __align__(128) unsigned char smem[];
-    float* outbuf = reinterpret_cast<float*>(smem + T::STAGES * T::STAGE_BYTES);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T::STAGES * T::STAGE_BYTES + T::OUT_BUFS * T::OUT_BYTES);
-    __shared__ int s_abort;
+    float* outbuf = reinterpret_cast<float*>(smem + STAGES * T::STAGE_BYTES);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * T::STAGE_BYTES + T::OUT_BUFS * T::OUT_BYTES);
+    // Abort flags, one per step parity: a flag is only ever set (on a bounded
+    // wait that expired) and is read by all threads after that step's barrier,
+    // so the decision to stop is uniform across the CTA.
+    __shared__ int s_abort[2];
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, g.Z);
     const int nplanes = z1 - z0 + 2;  // planes z0-1 .. z1
+    const int last = nplanes - 2;     // centre planes 1 .. last
     const int x = x0 + tx, y = y0 + ty;
     const bool active = x < g.X && y < g.Y;
+    const bool edge_xm = x == 0, edge_xp = x >= g.X - 1, edge_ym = y == 0, edge_yp = y >= g.Y - 1;
 
-    auto mask_of = [&](int p) -> const uint8_t* { return smem + (p % T::STAGES) * T::STAGE_BYTES; };
+    auto mask_of = [&](int p) -> const uint8_t* { return smem + (p % STAGES) * T::STAGE_BYTES; };
     auto plane_of = [&](int p) -> float* {
-        return reinterpret_cast<float*>(smem + (p % T::STAGES) * T::STAGE_BYTES + T::MASK_REGION);
+        return reinterpret_cast<float*>(smem + (p % STAGES) * T::STAGE_BYTES + T::MASK_REGION);
     };
     auto issue = [&](int p) {
-        uint64_t* bar = &bars[p % T::STAGES];
+        uint64_t* bar = &bars[p % STAGES];
         mbar_arrive_expect_tx(bar, T::PLANE_BYTES + T::MASK_BYTES);
         // Planes outside the grid are never read (walls use the centre
         // value), so they are loaded from a clamped in-grid z.
@@ -143,22 +239,35 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
         tma_load_3d(plane_of(p), &tm_src, (x0 - 1) * 12, y0 - 1, zz, bar);
         tma_load_3d((void*)mask_of(p), &tm_mask, x0 - 16, y0 - 1, zz, bar);
     };
+    auto is_source_plane = [&](int p) {
+        const int z = z0 - 1 + p;
+        return apply_sources && (z == 0 || z == g.Z - 1);
+    };
     auto transform = [&](int p) {  // boundary sources applied to a staged plane
         const int z = z0 - 1 + p;
-        if (z != 0 && z != g.Z - 1) return;
         float* P = plane_of(p);
         for (int i = tid; i < T::PW * T::PH; i += TX * TY) source_voxel(P + i * 12, z, g.Z, k);
     };
 
-    int issued = 0;
+    const int ci = ((ty + 1) * T::PW + (tx + 1)) * 12;  // own voxel in a staged plane
+    const int mi = (ty + 1) * T::MW + tx + 16;           // own column in a staged mask
+    // Wall flags of a centre plane: bit 0..3 = -x, +x, -y, +y neighbour reads the centre.
+    auto walls_of = [&](int p) -> uint32_t {
+        const uint8_t* M = mask_of(p);
+        return (uint32_t)(edge_xm || M[mi - 1]) | ((uint32_t)(edge_xp || M[mi + 1]) << 1) |
+               ((uint32_t)(edge_ym || M[mi - T::MW]) << 2) | ((uint32_t)(edge_yp || M[mi + T::MW]) << 3);
+    };
+
+    int issued = 0, waited = 0;
+    bool aborted = false;
     if (tid == 0) {
-        for (int s = 0; s < T::STAGES; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
-        s_abort = 0;
+        s_abort[0] = s_abort[1] = 0;
     }
     __syncthreads();
     if (tid == 0) {
-        const int pre = min(T::STAGES, nplanes);
+        const int pre = min(STAGES, nplanes);
         for (int p = 0; p < pre; ++p) issue(p);
         issued = pre;
     }
@@ -167,111 +276,108 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
     ok = mbar_wait_bounded(&bars[1], 0) && ok;
     if (!ok) {
         atomicOr(err, kErrTimeoutMbar);
-        s_abort = 1;
+        s_abort[0] = 1;
     }
+    waited = 2;
     __syncthreads();
-    int waited = 2;
-    if (!s_abort && apply_sources) {
-        transform(0);
-        transform(1);
-    }
-    __syncthreads();
-
-    const int ci = ((ty + 1) * T::PW + (tx + 1)) * 12;  // own voxel in a staged plane
-    const int mi = (ty + 1) * T::MW + tx + 16;           // own column in a staged mask
-    float below[12], cur[12], above[12];
-    bool mb = false, mc = false, ma = false;
-    if (!s_abort) {
-        load12(below, plane_of(0) + ci);
-        load12(cur, plane_of(1) + ci);
-        mb = mask_of(0)[mi] != 0;
-        mc = mask_of(1)[mi] != 0;
+    aborted = s_abort[0] != 0;
+    if (!aborted && apply_sources) {
+        if (is_source_plane(0)) transform(0);
+        if (is_source_plane(1)) transform(1);
     }
     __syncthreads();
 
-    for (int p = 1; p <= nplanes - 2 && !s_abort; ++p) {
+    Vox r0, r1, r2;
+    bool m0 = false, m1 = false, m2 = false;
+    uint32_t walls = 0;
+    if (!aborted) {
+        load_vox(r0, plane_of(0) + ci);
+        load_vox(r1, plane_of(1) + ci);
+        m0 = mask_of(0)[mi] != 0;
+        m1 = mask_of(1)[mi] != 0;
+        walls = walls_of(1);
+    }
+
+    // One centre plane p: B = below, C = centre, A receives the plane above.
+    auto step = [&](Vox& B, Vox& C, Vox& A, bool& mB, bool& mC, bool& mA, int p) -> bool {
         if (tid == 0) {
-            if (p + 3 < nplanes) {
+            if (p + STAGES - 1 < nplanes) {
                 fence_proxy_async_smem();
-                issue(p + 3);
-                issued = p + 4;
+                issue(p + STAGES - 1);
+                issued = p + STAGES;
             }
-            // the output buffer used now was last handed to a store two planes ago
-            bulk_wait_read<1>();
         }
-        if (!mbar_wait_bounded(&bars[(p + 1) % T::STAGES], ((p + 1) / T::STAGES) & 1)) {
+        if (!mbar_wait_bounded(&bars[(p + 1) % STAGES], ((p + 1) / STAGES) & 1)) {
             atomicOr(err, kErrTimeoutMbar);
-            s_abort = 1;
+            s_abort[p & 1] = 1;
         }
         waited = p + 2;
-        if (apply_sources) transform(p + 1);
-        __syncthreads();
-        if (s_abort) break;
+        if (is_source_plane(p + 1)) {  // uniform across the CTA
+            __syncthreads();
+            if (!s_abort[p & 1]) transform(p + 1);
+            __syncthreads();
+        }
+        // After an expired wait the staged data may be stale; the step still
+        // runs to its barrier (all reads stay inside shared memory) and the
+        // CTA stops after it.
 
-        load12(above, plane_of(p + 1) + ci);
-        ma = mask_of(p + 1)[mi] != 0;
+        load_vox(A, plane_of(p + 1) + ci);
+        mA = mask_of(p + 1)[mi] != 0;
+        const uint32_t next_walls = walls_of(p + 1);
 
         const int z = z0 - 1 + p;
         float out[12];
-        if (mc) {  // occupied: copied unchanged (field.rs:130-136)
+        if (mC) {  // occupied: copied unchanged (field.rs:130-136)
 #pragma unroll
-            for (int s = 0; s < 12; ++s) out[s] = cur[s];
+            for (int q = 0; q < 6; ++q) out[2 * q] = C.v[q].x, out[2 * q + 1] = C.v[q].y;
         } else {
             const float* P = plane_of(p);
-            const uint8_t* M = mask_of(p);
-            const float structural = cur[7];
-            const float niche = 1.0f - k.alpha_eps * structural / (k.k_eps + structural);
             // A wall or occupied neighbour reads as the centre value: point
             // its load at the centre voxel.
-            const float* pxm = (x == 0 || M[mi - 1]) ? P + ci : P + ci - 12;
-            const float* pxp = (x >= g.X - 1 || M[mi + 1]) ? P + ci : P + ci + 12;
-            const float* pym = (y == 0 || M[mi - T::MW]) ? P + ci : P + ci - T::ROWF;
-            const float* pyp = (y >= g.Y - 1 || M[mi + T::MW]) ? P + ci : P + ci + T::ROWF;
-            const bool wzm = z == 0 || mb;
-            const bool wzp = z >= g.Z - 1 || ma;
-            float nxm[12], nxp[12], nym[12], nyp[12];
-            load12(nxm, pxm);
-            load12(nxp, pxp);
-            load12(nym, pym);
-            load12(nyp, pyp);
-#pragma unroll
-            for (int s = 0; s < 12; ++s) {  // field.rs:152-195
-                const float c = cur[s];
-                const float d = k.d_voxel[s] * niche;
-                const float zm = wzm ? c : below[s];
-                const float zp = wzp ? c : above[s];
-                const float lap = nxm[s] + nxp[s] + nym[s] + nyp[s] + zm + zp - 6.0f * c;
-                const float decay = k.lambda_decay[s] * c;
-                const float nc = c + k.dt_sub * (d * lap - decay);
-                out[s] = fmaxf(nc, 0.0f);
-            }
+            Vox xm, xp, ym, yp;
+            load_vox(xm, P + ci - ((walls & 1u) ? 0 : 12));
+            load_vox(xp, P + ci + ((walls & 2u) ? 0 : 12));
+            load_vox(ym, P + ci - ((walls & 4u) ? 0 : T::ROWF));
+            load_vox(yp, P + ci + ((walls & 8u) ? 0 : T::ROWF));
+            stencil(out, C, xm, xp, ym, yp, B, A, z == 0 || mB, z >= g.Z - 1 || mA, k);
         }
-        float* ob = outbuf + (p & 1) * (T::OUT_BYTES / 4) + (ty * TX + tx) * 12;
+        float* ob = outbuf + (p % 3) * (T::OUT_BYTES / 4) + (ty * TX + tx) * 12;
         reinterpret_cast<float4*>(ob)[0] = make_float4(out[0], out[1], out[2], out[3]);
         reinterpret_cast<float4*>(ob)[1] = make_float4(out[4], out[5], out[6], out[7]);
         reinterpret_cast<float4*>(ob)[2] = make_float4(out[8], out[9], out[10], out[11]);
         if (c4_out && active) c4_out[((size_t)z * g.Y + y) * g.X + x] = out[4];
+        walls = next_walls;
         fence_proxy_async_smem();
         __syncthreads();
+        if (s_abort[p & 1]) {
+            aborted = true;
+            return false;
+        }
         if (tid == 0) {
-            tma_store_3d(&tm_dst, outbuf + (p & 1) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
+            tma_store_3d(&tm_dst, outbuf + (p % 3) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
             bulk_commit();
+            bulk_wait_read<1>();  // the store of plane p-1 has read its buffer
         }
-#pragma unroll
-        for (int s = 0; s < 12; ++s) {
-            below[s] = cur[s];
-            cur[s] = above[s];
+        return true;
+    };
+
+    if (!aborted) {
+        int p = 1;
+        bool go = true;
+        for (; go && p + 2 <= last; p += 3) {
+            go = step(r0, r1, r2, m0, m1, m2, p) && step(r1, r2, r0, m1, m2, m0, p + 1) &&
+                 step(r2, r0, r1, m2, m0, m1, p + 2);
         }
-        mb = mc;
-        mc = ma;
+        if (go && p <= last) go = step(r0, r1, r2, m0, m1, m2, p);
+        if (go && p + 1 <= last) go = step(r1, r2, r0, m1, m2, m0, p + 1);
     }
 
     if (tid == 0) {
         bulk_wait_all();
         // After an abort, wait (bounded) for loads still in flight so no copy
         // lands in shared memory after the CTA exits.
-        if (s_abort)
-            for (int q = waited; q < issued; ++q) mbar_wait_bounded(&bars[q % T::STAGES], (q / T::STAGES) & 1);
+        if (aborted)
+            for (int q = waited; q < issued; ++q) mbar_wait_bounded(&bars[q % STAGES], (q / STAGES) & 1);
     }
 }
 
@@ -393,41 +499,46 @@ __global__ void k_unpack_mask(const uint8_t* __restrict__ mask, uint8_t* __restr
 
 // ======================================================== launchers ======
 
-static const int kTileTY[] = {8, 16, 4, 32};
+// Tile table: (rows per tile, plane stages).  The autotuner picks one.
+static const int kTileTY[] = {8, 16, 4, 32, 8, 16, 4, 32};  // stages: 4 for tiles 0-3, 3 for 4-7
 
-int diffusion_tile_count() { return 4; }
+int diffusion_tile_count() { return 8; }
 
 void diffusion_tile_shape(int tile, int* tx, int* ty) {
     *tx = kDiffTX;
     *ty = kTileTY[tile];
 }
 
-template <int TY>
+template <int TY, int STAGES>
 static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
                                     int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
-    using T = DiffTile<TY>;
+    using T = DiffTile<TY, STAGES>;
     static int configured_device = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(k_diffuse<TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_diffuse<TY, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              T::SMEM_BYTES);
         if (e != cudaSuccess) return e;
         configured_device = dev;
     }
     dim3 grid((g.X + kDiffTX - 1) / kDiffTX, (g.Y + TY - 1) / TY, (g.Z + plan.zc - 1) / plan.zc);
-    k_diffuse<TY><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(plan.tm_load[which_src], plan.tm_store[which_src ^ 1],
-                                                            plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err);
+    k_diffuse<TY, STAGES><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(
+        plan.tm_load[which_src], plan.tm_store[which_src ^ 1], plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
                            int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
     switch (plan.tile) {
-        case 0: return launch_diffuse_t<8>(plan, which_src, g, k, apply_sources, c4_out, err, s);
-        case 1: return launch_diffuse_t<16>(plan, which_src, g, k, apply_sources, c4_out, err, s);
-        case 2: return launch_diffuse_t<4>(plan, which_src, g, k, apply_sources, c4_out, err, s);
-        default: return launch_diffuse_t<32>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 0: return launch_diffuse_t<8, 4>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 1: return launch_diffuse_t<16, 4>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 2: return launch_diffuse_t<4, 4>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 3: return launch_diffuse_t<32, 4>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 4: return launch_diffuse_t<8, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 5: return launch_diffuse_t<16, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 6: return launch_diffuse_t<4, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        default: return launch_diffuse_t<32, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
     }
 }
 
