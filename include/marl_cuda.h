@@ -297,11 +297,30 @@ marl_status marl_diffuse_tick_with_cells(marl_ctx* ctx, float* field, const uint
  * device memory.  field_dev holds the input and receives the output;
  * scratch_dev is a second buffer of the same size (the reference's
  * Field::scratch, crates/marl-field/src/field.rs:18-20); occupancy_dev is
- * one byte per voxel.  Stream-ordered on `cuda_stream` (NULL = legacy default
- * stream); no host synchronisation. */
+ * one byte per voxel.  The work is ordered on `cuda_stream` (NULL = legacy
+ * default stream); the call synchronizes that stream before returning so that
+ * device-side errors are reported. */
 marl_status marl_diffuse_device(float* field_dev, float* scratch_dev, const uint8_t* occupancy_dev,
                                 int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
                                 uint32_t substeps, void* cuda_stream);
+
+/* Allocation-free form of marl_diffuse_device (no counterpart in the
+ * reference).  For callers that must not allocate device memory while they
+ * run — their device memory belongs to another allocator or a fixed pool, or
+ * an allocation (and the synchronisation it can bring) is not acceptable in
+ * their loop.  It calls no cudaMalloc/cudaFree and no allocating library
+ * routine.  The ping-pong field copy, the padded occupancy mask and the error
+ * word live in one static device array that every GPU loading the library holds
+ * until exit (about 13 MiB).  Limits: at most 262,144 voxels, and
+ * Y * Z * (X rounded up to 16) <= 1,048,576 bytes of mask; larger grids get
+ * MARL_ERR_INVALID_INPUT.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and
+ * must not be issued.  Otherwise identical to marl_diffuse_device (same
+ * arguments minus scratch_dev, same results, synchronizes `cuda_stream`). */
+marl_status marl_diffuse_device_noalloc(float* field_dev, const uint8_t* occupancy_dev, int32_t gx, int32_t gy,
+                                        int32_t gz, const marl_sim_params* sim, uint32_t substeps,
+                                        void* cuda_stream);
 
 /* ---- formats ------------------------------------------------------------ */
 /* Canonical 536-byte ruleset payload (crates/marl-format/src/lib.rs:70-89). */

@@ -139,6 +139,7 @@ EXPORTED = [
     "marl_upload_cells", "marl_download_cells", "marl_cell_count", "marl_download_occupancy",
     "marl_apply_boundary_sources", "marl_diffuse", "marl_light_update", "marl_cell_phase", "marl_tick",
     "marl_apply_edits", "marl_mass_f64", "marl_diffuse_tick_with_cells", "marl_diffuse_device",
+    "marl_diffuse_device_noalloc",
     "marl_ruleset_pack_canonical", "marl_ruleset_unpack_canonical",
     "marl_engine_create", "marl_engine_create_from_state", "marl_engine_destroy", "marl_engine_set_stream",
     "marl_engine_step", "marl_engine_stats_get", "marl_engine_get_cells", "marl_engine_get_field",
@@ -187,6 +188,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_mass_f64": (c_int32, [P, P]),
         "marl_diffuse_tick_with_cells": (c_int32, [P, P, P]),
         "marl_diffuse_device": (c_int32, [P, P, P, c_int32, c_int32, c_int32, POINTER(SimParams), c_uint32, P]),
+        "marl_diffuse_device_noalloc": (c_int32, [P, P, c_int32, c_int32, c_int32, POINTER(SimParams), c_uint32, P]),
         "marl_ruleset_pack_canonical": (c_int32, [P, P]),
         "marl_ruleset_unpack_canonical": (c_int32, [P, P]),
         "marl_engine_create": (c_int32, [c_int32, c_int32, c_int32, POINTER(SimParams), c_uint64, c_uint32, c_uint32,
@@ -411,6 +413,20 @@ def diffuse_device(field_ptr: int, scratch_ptr: int, occ_ptr: int, dims, params:
     X, Y, Z = dims
     _check(lib.marl_diffuse_device(c_void_p(field_ptr), c_void_p(scratch_ptr), c_void_p(occ_ptr), X, Y, Z,
                                    ctypes.byref(params), substeps, c_void_p(stream_ptr)), "marl_diffuse_device")
+
+
+def diffuse_device_noalloc(field_ptr: int, occ_ptr: int, dims, params: SimParams, substeps: int,
+                           stream_ptr: int = 0) -> None:
+    """marl_diffuse_device_noalloc: like diffuse_device, but with no device allocation at all.
+
+    For callers that must not allocate device memory while they run.  Its
+    scratch (about 13 MiB) is a static device array shared by every call, so
+    calls must not overlap on the GPU; grids are limited to 262,144 voxels.
+    """
+    lib = load()
+    X, Y, Z = dims
+    _check(lib.marl_diffuse_device_noalloc(c_void_p(field_ptr), c_void_p(occ_ptr), X, Y, Z, ctypes.byref(params),
+                                           substeps, c_void_p(stream_ptr)), "marl_diffuse_device_noalloc")
 
 
 def pack_ruleset(rs: np.ndarray) -> bytes:
