@@ -145,22 +145,32 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
     const uint32_t st0 = pre.state;
     const float light = pre.light;
 
-    // Gather: mean of the empty face neighbours (spatial.rs:56-77).
+    // Gather: mean of the empty face neighbours (spatial.rs:56-77), summed in
+    // face order from 0.0.  Dividing by n = 1, 2 or 4 is done as an exact
+    // multiplication (a power-of-two divisor gives the identical IEEE result).
+    float acc[12];
 #pragma unroll
-    for (int s = 0; s < 12; ++s) S.ext[s][tid] = 0.0f;
+    for (int s = 0; s < 12; ++s) acc[s] = 0.0f;
+#pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (!((nb >> f) & 1u)) continue;
         const float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
         const float4 q0 = ld4(v), q1 = ld4(v + 4), q2 = ld4(v + 8);
         const float vals[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 #pragma unroll
-        for (int s = 0; s < 12; ++s) S.ext[s][tid] = S.ext[s][tid] + vals[s];
+        for (int s = 0; s < 12; ++s) acc[s] = acc[s] + vals[s];
     }
-    if (n > 0) {
+    if (n == 2 || n == 4) {
+        const float inv = n == 2 ? 0.5f : 0.25f;
+#pragma unroll
+        for (int s = 0; s < 12; ++s) acc[s] = acc[s] * inv;
+    } else if (n > 1) {
         const float nf = (float)n;
 #pragma unroll
-        for (int s = 0; s < 12; ++s) S.ext[s][tid] = S.ext[s][tid] / nf;
+        for (int s = 0; s < 12; ++s) acc[s] = acc[s] / nf;
     }
+#pragma unroll
+    for (int s = 0; s < 12; ++s) S.ext[s][tid] = acc[s];
 
     // CellState::tick (cell.rs:193-369).  Phase 1 (receptors) only writes an
     // unused local and is omitted.
@@ -170,18 +180,26 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
     const float dt = c.dt;
     cp_async_wait_all();
 
-    // Phase 2: transport (cell.rs:223-238)
+    // Phase 2: transport (cell.rs:223-238).  Uptake depends only on the
+    // gathered environment, so all eight are evaluated first; secretion
+    // follows the internal state transporter by transporter.
     const uint4 tpi = S.idx[0][tid];
     const uint32_t tpw[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
+    float uptakes[MARL_S_TRANSPORTERS];
+#pragma unroll
+    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
+        const uint32_t e = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFu;
+        const float ev = e < MARL_S_EXT ? S.ext[e][tid] : 0.0f;
+        uptakes[i] = S.tp[i][tid].x * ev / (1.0f + ev);
+    }
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
         const uint32_t pair = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
         const uint32_t e = pair & 0xFF, k = pair >> 8;
         if (e >= MARL_S_EXT || k >= MARL_M_INT) continue;
         const float2 r = S.tp[i][tid];
-        const float ev = S.ext[e][tid];
         const float xk = S.x[k][tid];
-        const float uptake = r.x * ev / (1.0f + ev);
+        const float uptake = uptakes[i];
         const float secretion = r.y * xk / (1.0f + xk);
         S.x[k][tid] = rclamp(xk + (uptake - secretion) * dt, 0.0f, c.c_max);
         S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
@@ -284,14 +302,30 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
     // Scatter: split deltas over the same neighbours, clamp after each add
     // (spatial.rs:87-110, field.rs:57-62).
     if (n > 0) {
-        const float nf = (float)n;
-        float split[12];
+        // The neighbours' current values are loaded together before any
+        // store: no other cell touches N(j) while this cell holds it.
+        float4 nv[6][3];
 #pragma unroll
-        for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] / nf;
+        for (int f = 0; f < 6; ++f) {
+            if (!((nb >> f) & 1u)) continue;
+            const float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
+            nv[f][0] = ld4(v), nv[f][1] = ld4(v + 4), nv[f][2] = ld4(v + 8);
+        }
+        float split[12];
+        if (n == 1 || n == 2 || n == 4) {
+            const float inv = n == 1 ? 1.0f : (n == 2 ? 0.5f : 0.25f);
+#pragma unroll
+            for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] * inv;
+        } else {
+            const float nf = (float)n;
+#pragma unroll
+            for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] / nf;
+        }
+#pragma unroll
         for (int f = 0; f < 6; ++f) {
             if (!((nb >> f) & 1u)) continue;
             float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
-            float4 q0 = ld4(v), q1 = ld4(v + 4), q2 = ld4(v + 8);
+            float4 q0 = nv[f][0], q1 = nv[f][1], q2 = nv[f][2];
             q0 = make_float4(fmaxf(q0.x + split[0], 0.0f), fmaxf(q0.y + split[1], 0.0f), fmaxf(q0.z + split[2], 0.0f),
                              fmaxf(q0.w + split[3], 0.0f));
             q1 = make_float4(fmaxf(q1.x + split[4], 0.0f), fmaxf(q1.y + split[5], 0.0f), fmaxf(q1.z + split[6], 0.0f),
