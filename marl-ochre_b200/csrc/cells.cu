@@ -167,7 +167,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
     } else if (n > 1) {
         const float nf = (float)n;
 #pragma unroll
-        for (int s = 0; s < 12; ++s) acc[s] = acc[s] / nf;
+        for (int s = 0; s < 12; ++s) acc[s] = div_rn(acc[s], nf);
     }
 #pragma unroll
     for (int s = 0; s < 12; ++s) S.ext[s][tid] = acc[s];
@@ -190,7 +190,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
         const uint32_t e = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFu;
         const float ev = e < MARL_S_EXT ? S.ext[e][tid] : 0.0f;
-        uptakes[i] = S.tp[i][tid].x * ev / (1.0f + ev);
+        uptakes[i] = div_rn(S.tp[i][tid].x * ev, 1.0f + ev);
     }
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
@@ -200,7 +200,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
         const float2 r = S.tp[i][tid];
         const float xk = S.x[k][tid];
         const float uptake = uptakes[i];
-        const float secretion = r.y * xk / (1.0f + xk);
+        const float secretion = div_rn(r.y * xk, 1.0f + xk);
         S.x[k][tid] = rclamp(xk + (uptake - secretion) * dt, 0.0f, c.c_max);
         S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
     }
@@ -220,12 +220,12 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
         if (si >= MARL_M_INT || pi >= MARL_M_INT || ci >= MARL_M_INT) continue;
         const float s = S.x[si][tid];
         const float cc = S.x[ci][tid];
-        const float substrate_term = s / (km + s + feps);
-        const float catalyst_term = c.epsilon + cc / (kcat + cc + feps);
+        const float substrate_term = div_rn(s, km + s + feps);
+        const float catalyst_term = c.epsilon + div_rn(cc, kcat + cc + feps);
         float rate = vmax * substrate_term * catalyst_term;
         if (fi != MARL_NO_COFACTOR && fi < MARL_M_INT) {
             const float cof = S.x[fi][tid];
-            rate *= cof / (1.0f + cof);
+            rate *= div_rn(cof, 1.0f + cof);
             const float consumed = fminf(0.5f * rate * dt, S.x[fi][tid]);
             S.x[fi][tid] = S.x[fi][tid] - consumed;
         }
@@ -264,7 +264,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
             const float2 pr = S.ef[i][tid];
             const float xk = S.x[k][tid];
             if (xk > pr.x) {
-                const float amount = pr.y * xk / (1.0f + xk) * dt;
+                const float amount = div_rn(pr.y * xk, 1.0f + xk) * dt;
                 S.x[k][tid] = fmaxf(xk - amount, 0.0f);
                 S.del[e][tid] = S.del[e][tid] + amount;
             }
@@ -319,7 +319,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
         } else {
             const float nf = (float)n;
 #pragma unroll
-            for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] / nf;
+            for (int s = 0; s < 12; ++s) split[s] = div_rn(S.del[s][tid], nf);
         }
 #pragma unroll
         for (int f = 0; f < 6; ++f) {

@@ -136,7 +136,7 @@ __device__ __forceinline__ void stencil(float out[12], const Vox& c, const Vox& 
                                         const Vox& yp, const Vox& below, const Vox& above, bool wzm, bool wzp,
                                         const FieldConsts& k) {
     const float structural = c.v[3].y;  // species 7
-    const float niche = 1.0f - k.alpha_eps * structural / (k.k_eps + structural);
+    const float niche = 1.0f - div_rn(k.alpha_eps * structural, k.k_eps + structural);
 #if MARL_STENCIL_MODE == 0
     // Scalar IEEE operations (no contraction possible).
 #pragma unroll
