@@ -175,13 +175,17 @@ def run_reference(args) -> int:
     return 0
 
 
-def diffusion_roofline(marl, torch, engine, stream) -> dict:
+def diffusion_roofline(marl, torch, engine, stream, fixed_tile=None) -> dict:
     """Times the diffusion substep on the engine's current state with CUDA events."""
     ctx = marl.Context(DIMS, engine.params, cell_capacity=max(int(engine.stats()["population"]), 1) + 16)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload_field(engine.field())
     ctx.upload_cells(engine.cells())
-    us = ctx.autotune(5)
+    if fixed_tile is None:
+        us = ctx.autotune(5)
+    else:
+        ctx.set_tile(*fixed_tile)
+        us = None
     tile, zc = ctx.get_tile()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     groups, per_group = 20, 10
@@ -222,6 +226,9 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile", type=int, nargs=2, metavar=("TILE", "ZC"),
+                    help="fixed diffusion tile index and z-chunk instead of the autotuner (for launch lists)")
+    ap.add_argument("--no-roofline", action="store_true", help="skip the separate diffusion timing")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -248,7 +255,11 @@ def main() -> int:
 
     eng = marl.Engine(DIMS, marl.default_params(), rng_seed=SEED, seed_count=SEED_COUNT, cell_capacity=1 << 20)
     eng.set_stream(stream.cuda_stream)
-    eng.autotune(5)
+    if args.tile:
+        lib = marl.load()
+        marl._check(lib.marl_ctx_set_tile(lib.marl_engine_ctx(eng.h), args.tile[0], args.tile[1]), "set_tile")
+    else:
+        eng.autotune(5)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     eng.step(args.warmup)
     pop0 = eng.stats()["population"]
@@ -286,7 +297,9 @@ def main() -> int:
     value = total_ticks / dev_s
     e2e = total_ticks / wall
 
-    roof = diffusion_roofline(marl, torch, eng, stream) if rank == 0 else None
+    roof = None
+    if rank == 0 and not args.no_roofline:
+        roof = diffusion_roofline(marl, torch, eng, stream, tuple(args.tile) if args.tile else None)
     if rank == 0:
         base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline()
         line = {

@@ -363,6 +363,51 @@ marl_status marl_engine_get_field(marl_engine* e, float* field);
 marl_status marl_engine_get_light(marl_engine* e, float* light);
 marl_ctx* marl_engine_ctx(marl_engine* e);
 
+/* ---- batch: many independent runs advanced together --------------------
+ * No counterpart in the reference, which advances one run per process
+ * (crates/marl-sim/src/lib.rs:34-277).  Each run of a batch behaves exactly
+ * like a marl_engine created with the same grid, parameters, rng_seed and
+ * seed_count: same field, cells and change lists, bit for bit.  The runs may
+ * have different grid sizes.  Every device phase of a tick (diffusion
+ * substeps, light, the cell loop, compaction) is one kernel launch covering
+ * all runs, and the device part of a tick is replayed from a CUDA graph; fate
+ * processing runs on the host, one run per worker thread.  All runs share
+ * `sim`.  Not thread-safe; one stream. */
+typedef struct marl_batch marl_batch;
+
+typedef struct marl_run_spec {
+    int32_t gx, gy, gz;
+    uint32_t seed_count;     /* cells per starter metabolism */
+    uint64_t rng_seed;
+    uint32_t cell_capacity;  /* 0: X*Y*Z/4, at least 1024 */
+    uint32_t _pad;
+} marl_run_spec;
+
+marl_status marl_batch_create(const marl_run_spec* runs, uint32_t n_runs, const marl_sim_params* sim,
+                              marl_batch** out);
+void marl_batch_destroy(marl_batch* b);
+/* NULL = legacy default stream.  The tick graphs are rebuilt lazily. */
+marl_status marl_batch_set_stream(marl_batch* b, void* cuda_stream);
+/* Host threads for fate processing (0: hardware concurrency, capped at 64). */
+marl_status marl_batch_set_host_threads(marl_batch* b, int32_t threads);
+/* Diffusion tile choice shared by all runs (indices as marl_ctx_set_tile). */
+marl_status marl_batch_set_tile(marl_batch* b, int32_t tile, int32_t zc);
+marl_status marl_batch_get_tile(marl_batch* b, int32_t* tile, int32_t* zc);
+/* Times `reps` batched substeps for every tile candidate and keeps the
+ * fastest; the runs' fields are not modified. */
+marl_status marl_batch_autotune(marl_batch* b, int32_t reps, float* best_us_per_substep);
+/* use_graph = 0 launches the device tick kernel by kernel instead of
+ * replaying the captured graph (same results). */
+marl_status marl_batch_set_graph(marl_batch* b, int32_t use_graph);
+marl_status marl_batch_step(marl_batch* b, uint32_t ticks);
+marl_status marl_batch_run_count(marl_batch* b, uint32_t* n_runs);
+marl_status marl_batch_stats_get(marl_batch* b, uint32_t run, marl_engine_stats* out);
+marl_status marl_batch_get_cells(marl_batch* b, uint32_t run, marl_cell* out, uint32_t cap, uint32_t* n_out);
+marl_status marl_batch_get_field(marl_batch* b, uint32_t run, float* field);
+marl_status marl_batch_get_light(marl_batch* b, uint32_t run, float* light);
+/* As marl_ctx_counters, over the whole batch (ticks counts batch ticks). */
+marl_status marl_batch_counters(marl_batch* b, marl_counters* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -30,9 +30,8 @@ namespace marl {
 __constant__ int c_face[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
 
 // ---------------------------------------------------------- schedule -----
-__global__ void k_cell_schedule(CellTable t, uint32_t n, Grid g, const int32_t* __restrict__ cmap) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+__device__ __forceinline__ void schedule_cell(const CellTable& t, const Grid g, const int32_t* __restrict__ cmap,
+                                              const uint32_t j) {
     const uint32_t P = t.pos[j];
     const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
     uint32_t nb = 0;
@@ -55,6 +54,35 @@ __global__ void k_cell_schedule(CellTable t, uint32_t n, Grid g, const int32_t* 
         t.dep[(size_t)f * t.cap + j] = dep;
     }
     t.nb[j] = nb;
+}
+
+__global__ void k_cell_schedule(CellTable t, uint32_t n, Grid g, const int32_t* __restrict__ cmap) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) schedule_cell(t, g, cmap, j);
+}
+
+// Run of the batch that global cell index `gi` belongs to (runs are stored in
+// ascending cell_base order).
+__device__ __forceinline__ int find_run(const RunDesc* __restrict__ runs, int n_runs, uint32_t gi) {
+    int lo = 0, hi = n_runs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (runs[mid].cell_base <= gi) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t batch_total(const RunDesc* __restrict__ runs, int n_runs) {
+    return runs[n_runs - 1].cell_base + runs[n_runs - 1].n;
+}
+
+__global__ void k_cell_schedule_batch(const RunDesc* __restrict__ runs, int n_runs) {
+    const uint32_t total = batch_total(runs, n_runs);
+    for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total; gi += gridDim.x * blockDim.x) {
+        const int r = find_run(runs, n_runs, gi);
+        const RunDesc& R = runs[r];
+        schedule_cell(R.t, R.g, R.cmap, gi - R.cell_base);
+    }
 }
 
 // ------------------------------------------------------------ update -----
@@ -105,9 +133,18 @@ struct CellPre {
     int32_t dep[6];
 };
 
-__device__ __forceinline__ void stage_cell(const CellLaunch& a, CellScratch& S, uint32_t j, CellPre& pre) {
+// What one lane needs to know about the run its cell belongs to.
+struct CellRunView {
+    const CellTable* t;
+    Grid g;
+    float* field;
+    const float* light;
+    uint32_t epoch;
+};
+
+__device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j, CellPre& pre) {
     const int tid = threadIdx.x;
-    const CellTable& t = a.t;
+    const CellTable& t = *v.t;
     const size_t cap = t.cap;
     // Ruleset and internal state: asynchronous copies into shared memory.
 #pragma unroll
@@ -126,15 +163,16 @@ __device__ __forceinline__ void stage_cell(const CellLaunch& a, CellScratch& S, 
     pre.state = t.state[j];
 #pragma unroll
     for (int f = 0; f < 6; ++f) pre.dep[f] = ((pre.nb >> f) & 1u) ? t.dep[(size_t)f * cap + j] : -1;
-    const Grid g = a.g;
-    pre.light = a.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
+    const Grid g = v.g;
+    pre.light = v.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
 }
 
 // Gather -> tick -> scatter of cell j, after all its dependencies are done.
-__device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, const CellPre& pre) {
+__device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
+                            const CellPre& pre) {
     const int tid = threadIdx.x;
-    const CellTable& t = a.t;
-    const Grid g = a.g;
+    const CellTable& t = *v.t;
+    const Grid g = v.g;
     const uint32_t nb = pre.nb;
     const uint32_t P = pre.pos;
     const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
@@ -154,8 +192,8 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (!((nb >> f) & 1u)) continue;
-        const float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
-        const float4 q0 = ld4(v), q1 = ld4(v + 4), q2 = ld4(v + 8);
+        const float* src = v.field + (size_t)((long long)vox + off[f]) * 12;
+        const float4 q0 = ld4(src), q1 = ld4(src + 4), q2 = ld4(src + 8);
         const float vals[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 #pragma unroll
         for (int s = 0; s < 12; ++s) acc[s] = acc[s] + vals[s];
@@ -176,7 +214,6 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
     // unused local and is omitted.
 #pragma unroll
     for (int s = 0; s < 12; ++s) S.del[s][tid] = 0.0f;
-    const CellConsts& c = a.k;
     const float dt = c.dt;
     cp_async_wait_all();
 
@@ -308,8 +345,8 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
             if (!((nb >> f) & 1u)) continue;
-            const float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
-            nv[f][0] = ld4(v), nv[f][1] = ld4(v + 4), nv[f][2] = ld4(v + 8);
+            const float* src = v.field + (size_t)((long long)vox + off[f]) * 12;
+            nv[f][0] = ld4(src), nv[f][1] = ld4(src + 4), nv[f][2] = ld4(src + 8);
         }
         float split[12];
         if (n == 1 || n == 2 || n == 4) {
@@ -324,7 +361,7 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
             if (!((nb >> f) & 1u)) continue;
-            float* v = a.field + (size_t)((long long)vox + off[f]) * 12;
+            float* dst = v.field + (size_t)((long long)vox + off[f]) * 12;
             float4 q0 = nv[f][0], q1 = nv[f][1], q2 = nv[f][2];
             q0 = make_float4(fmaxf(q0.x + split[0], 0.0f), fmaxf(q0.y + split[1], 0.0f), fmaxf(q0.z + split[2], 0.0f),
                              fmaxf(q0.w + split[3], 0.0f));
@@ -332,49 +369,57 @@ __device__ void update_cell(const CellLaunch& a, CellScratch& S, uint32_t j, con
                              fmaxf(q1.w + split[7], 0.0f));
             q2 = make_float4(fmaxf(q2.x + split[8], 0.0f), fmaxf(q2.y + split[9], 0.0f),
                              fmaxf(q2.z + split[10], 0.0f), fmaxf(q2.w + split[11], 0.0f));
-            st4(v, q0);
-            st4(v + 4, q1);
-            st4(v + 8, q2);
+            st4(dst, q0);
+            st4(dst + 4, q1);
+            st4(dst + 8, q2);
         }
     }
 }
 
-__global__ void __launch_bounds__(kTickThreads) k_cell_tick(CellLaunch a) {
-    extern __shared__ __align__(16) unsigned char tick_smem[];
-    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
+// The ticket loop shared by the single-run and the batched kernel.  `resolve`
+// maps a ticket (global cell index) to the lane's run view and local index.
+template <class Resolve>
+__device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts& c, uint32_t total, uint32_t* ticket,
+                                               uint32_t* err, Resolve resolve) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
-    const CellTable& t = a.t;
     for (;;) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(a.ticket, 32u);
+        if (lane == 0) base = atomicAdd(ticket, 32u);
         base = __shfl_sync(FULL, base, 0);
-        if (base >= a.n) break;
-        const uint32_t j = base + lane;
-        bool pending = j < a.n;
+        if (base >= total) break;
+        const uint32_t gi = base + lane;
+        bool pending = gi < total;
+        CellRunView v{};
+        uint32_t j = 0;
         CellPre pre;
-        if (pending) stage_cell(a, S, j, pre);
+        if (pending) {
+            resolve(gi, v, j);
+            stage_cell(v, S, j, pre);
+        }
         uint32_t spins = 0;
         while (__any_sync(FULL, pending)) {
             if (pending) {
+                const CellTable& t = *v.t;
                 bool ready = true;
 #pragma unroll
                 for (int f = 0; f < 6; ++f)
-                    if (pre.dep[f] >= 0 && ld_acquire_u32(&t.done[pre.dep[f]]) != a.epoch) ready = false;
+                    if (pre.dep[f] >= 0 && ld_acquire_u32(&t.done[pre.dep[f]]) != v.epoch) ready = false;
                 if (ready) {
-                    update_cell(a, S, j, pre);
+                    update_cell(v, c, S, j, pre);
                     // release: this cell's field writes are visible before its done flag
-                    st_release_u32(&t.done[j], a.epoch);
+                    st_release_u32(&t.done[j], v.epoch);
                     pending = false;
                 }
             }
             if (__any_sync(FULL, pending)) {
                 if (++spins > kFlagSpinLimit) {
                     if (pending) {
-                        atomicOr(a.err, kErrTimeoutDeps);
+                        const CellTable& t = *v.t;
+                        atomicOr(err, kErrTimeoutDeps);
                         cp_async_wait_all();  // drain this lane's staging copies
                         t.events[j] = MARL_EVENT_NONE;
-                        st_release_u32(&t.done[j], a.epoch);
+                        st_release_u32(&t.done[j], v.epoch);
                         pending = false;
                     }
                 } else {
@@ -383,6 +428,30 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(CellLaunch a) {
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constant__ CellLaunch a) {
+    extern __shared__ __align__(16) unsigned char tick_smem[];
+    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
+    cell_tick_loop(S, a.k, a.n, a.ticket, a.err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch};
+        j = gi;
+    });
+}
+
+// Batched form: tickets run over the cells of all runs, run-major (run r's
+// cell j is ticket cell_base(r) + j), so every dependency of a cell, which lies
+// in the same run at a smaller index, also has a smaller ticket.
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc* __restrict__ runs, int n_runs,
+                                                                  BatchScalars* __restrict__ bs, CellConsts c,
+                                                                  int parity) {
+    extern __shared__ __align__(16) unsigned char tick_smem[];
+    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
+    cell_tick_loop(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+        const RunDesc& R = runs[find_run(runs, n_runs, gi)];
+        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch};
+        j = gi - R.cell_base;
+    });
 }
 
 // -------------------------------------------------------- compaction -----
@@ -464,6 +533,84 @@ __global__ void __launch_bounds__(kCompactThreads) k_scatter_events(CellTable t,
     }
 }
 
+// Batched compaction: block r compacts run r's events chunk by chunk in cell
+// order, carrying the running offset, into that run's change list.
+__global__ void __launch_bounds__(kCompactThreads) k_compact_batch(const RunDesc* __restrict__ runs) {
+    __shared__ uint32_t warp_tot[kCompactThreads / 32];
+    __shared__ uint32_t s_off;
+    const RunDesc& R = runs[blockIdx.x];
+    const CellTable& t = R.t;
+    const uint32_t n = R.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_off = 0;
+    __syncthreads();
+    for (uint32_t chunk = 0; chunk < n; chunk += kCompactPerBlock) {
+        const uint32_t first = chunk + threadIdx.x * kCompactPerThread;
+        uint32_t flags = 0, cnt = 0;
+#pragma unroll
+        for (int i = 0; i < kCompactPerThread; ++i)
+            if (first + i < n && is_change(t.events[first + i])) {
+                flags |= 1u << i;
+                ++cnt;
+            }
+        uint32_t incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        uint32_t warp_off = 0, block_tot = 0;
+        for (int w = 0; w < kCompactThreads / 32; ++w) {
+            if (w < warp) warp_off += warp_tot[w];
+            block_tot += warp_tot[w];
+        }
+        uint32_t pos = s_off + warp_off + incl - cnt;
+        for (int i = 0; i < kCompactPerThread; ++i) {
+            if (!((flags >> i) & 1u)) continue;
+            const uint32_t j = first + i;
+            if (pos < R.change_cap) {
+                marl_change& c = R.changes[pos];
+                c.cell = j;
+                c.event = t.events[j];
+                c.quiescent = (uint8_t)((t.state[j] >> 16) & 1u);
+                c._pad = 0;
+                for (int k = 0; k < MARL_M_INT; ++k) c.internal[k] = t.internal[(size_t)k * t.cap + j];
+            }
+            ++pos;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_off += block_tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        R.hdr->count = s_off;
+        R.hdr->n_cells = n;
+    }
+}
+
+// Block r copies run r's change list behind those of runs < r.
+__global__ void __launch_bounds__(256) k_pack_changes(const RunDesc* __restrict__ runs, int n_runs,
+                                                      BatchScalars* __restrict__ bs, marl_change* __restrict__ packed) {
+    __shared__ uint32_t red[256];
+    uint32_t part = 0;
+    for (int q = threadIdx.x; q < (int)blockIdx.x; q += 256) part += min(runs[q].hdr->count, runs[q].change_cap);
+    red[threadIdx.x] = part;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const uint32_t off = red[0];
+    const RunDesc& R = runs[blockIdx.x];
+    const uint32_t cnt = min(R.hdr->count, R.change_cap);
+    const uint32_t words = cnt * (uint32_t)(sizeof(marl_change) / 4);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(R.changes);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(packed + off);
+    for (uint32_t i = threadIdx.x; i < words; i += 256) dst[i] = src[i];
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) bs->changes = off + cnt;
+}
+
 // ------------------------------------------------------------- edits -----
 __device__ void write_record(CellTable& t, uint32_t slot, const marl_cell& c) {
     const size_t cap = t.cap;
@@ -506,21 +653,31 @@ __device__ void write_record(CellTable& t, uint32_t slot, const marl_cell& c) {
     cold[25] = r.mutation_rate;
 }
 
-__global__ void k_cells_from_records(const marl_cell* __restrict__ rec, uint32_t count, uint32_t base, CellTable t,
-                                     Grid g, int32_t* __restrict__ cmap, uint8_t* __restrict__ mask,
-                                     uint32_t* err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    const marl_cell& c = rec[i];
+__device__ __forceinline__ void birth_one(CellTable t, const Grid g, int32_t* cmap, uint8_t* mask, uint32_t slot,
+                                          const marl_cell& c, uint32_t* err) {
     if (c.pos[0] >= g.X || c.pos[1] >= g.Y || c.pos[2] >= g.Z) {
         atomicOr(err, kErrBadIndex);
         return;
     }
-    const uint32_t slot = base + i;
     write_record(t, slot, c);
     const size_t row = (size_t)c.pos[2] * g.Y + c.pos[1];
     cmap[row * g.X + c.pos[0]] = (int32_t)slot;
     mask[row * mask_pitch(g.X) + c.pos[0]] = 1;
+}
+
+__global__ void k_cells_from_records(const marl_cell* __restrict__ rec, uint32_t count, uint32_t base, CellTable t,
+                                     Grid g, int32_t* __restrict__ cmap, uint8_t* __restrict__ mask,
+                                     uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) birth_one(t, g, cmap, mask, base + i, rec[i], err);
+}
+
+__global__ void k_births_batch(const RunDesc* __restrict__ runs, const marl_cell* __restrict__ recs,
+                               const uint2* __restrict__ slots, uint32_t count, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const RunDesc& R = runs[slots[i].x];
+    birth_one(R.t, R.g, R.cmap, R.mask, slots[i].y, recs[i], err);
 }
 
 __global__ void k_cells_to_records(CellTable t, uint32_t n, marl_cell* __restrict__ rec) {
@@ -589,36 +746,53 @@ __global__ void k_cells_to_records(CellTable t, uint32_t n, marl_cell* __restric
 }
 
 // Division halving (crates/marl-sim/src/lib.rs:237-240): parent internals *= 0.5.
-__global__ void k_halve(CellTable t, const uint32_t* __restrict__ idx, uint32_t count) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count * MARL_M_INT) return;
-    const uint32_t p = idx[i / MARL_M_INT];
-    const uint32_t k = i % MARL_M_INT;
+__device__ __forceinline__ void halve_one(const CellTable& t, uint32_t p, uint32_t k) {
     float& v = t.internal[(size_t)k * t.cap + p];
     v = v * 0.5f;
 }
 
-// Dead cells leave the occupancy (cell_map.remove, lib.rs:261-262).
-__global__ void k_clear_dead(CellTable t, const uint32_t* __restrict__ idx, uint32_t count, Grid g,
-                             int32_t* __restrict__ cmap, uint8_t* __restrict__ mask) {
+__global__ void k_halve(CellTable t, const uint32_t* __restrict__ idx, uint32_t count) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    const uint32_t P = t.pos[idx[i]];
+    if (i >= count * MARL_M_INT) return;
+    halve_one(t, idx[i / MARL_M_INT], i % MARL_M_INT);
+}
+
+__global__ void k_halve_batch(const RunDesc* __restrict__ runs, const uint2* __restrict__ items, uint32_t count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count * MARL_M_INT) return;
+    const uint2 it = items[i / MARL_M_INT];
+    halve_one(runs[it.x].t, it.y, i % MARL_M_INT);
+}
+
+// Dead cells leave the occupancy (cell_map.remove, lib.rs:261-262).
+__device__ __forceinline__ void clear_dead_one(const CellTable& t, const Grid g, int32_t* cmap, uint8_t* mask,
+                                               uint32_t idx) {
+    const uint32_t P = t.pos[idx];
     const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
     cmap[row * g.X + pos_x(P)] = -1;
     mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
 }
 
+__global__ void k_clear_dead(CellTable t, const uint32_t* __restrict__ idx, uint32_t count, Grid g,
+                             int32_t* __restrict__ cmap, uint8_t* __restrict__ mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) clear_dead_one(t, g, cmap, mask, idx[i]);
+}
+
+__global__ void k_clear_dead_batch(const RunDesc* __restrict__ runs, const uint2* __restrict__ items, uint32_t count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const RunDesc& R = runs[items[i].x];
+    clear_dead_one(R.t, R.g, R.cmap, R.mask, items[i].y);
+}
+
 // swap_remove result (lib.rs:258-267): slot dst receives the cell in slot src.
 // Sources are >= the post-death length and destinations below it, so the
 // copies are independent.
-__global__ void k_moves(CellTable t, const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t count,
-                        Grid g, int32_t* __restrict__ cmap) {
-    // One warp per move; each lane copies a few words, all loads first.
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int l = threadIdx.x & 31;
-    if (i >= count) return;
-    const uint32_t d = dst[i], s = src[i];
+// One warp per move: lane l copies a few words of slot s into slot d, all
+// loads before any store.
+__device__ __forceinline__ void move_one(const CellTable& t, const Grid g, int32_t* cmap, uint32_t d, uint32_t s,
+                                         int l) {
     const size_t cap = t.cap;
     uint4 rx = make_uint4(0, 0, 0, 0);
     float in = 0.0f, cold = 0.0f;
@@ -646,6 +820,20 @@ __global__ void k_moves(CellTable t, const uint32_t* __restrict__ dst, const uin
     if (l == 28) t.tp_idx[d] = w;
     if (l == 29) t.ef_idx[d] = w;
     if (l == 30) t.fate[d] = fate;
+}
+
+__global__ void k_moves(CellTable t, const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t count,
+                        Grid g, int32_t* __restrict__ cmap) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i < count) move_one(t, g, cmap, dst[i], src[i], threadIdx.x & 31);
+}
+
+__global__ void k_moves_batch(const RunDesc* __restrict__ runs, const uint4* __restrict__ items, uint32_t count) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= count) return;
+    const uint4 it = items[i];
+    const RunDesc& R = runs[it.x];
+    move_one(R.t, R.g, R.cmap, it.y, it.z, threadIdx.x & 31);
 }
 
 __global__ void k_rebuild_maps(CellTable t, uint32_t n, Grid g, int32_t* __restrict__ cmap,
@@ -737,6 +925,66 @@ cudaError_t launch_rebuild_maps(const CellTable& t, uint32_t n, const Grid& g, i
                                 cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_rebuild_maps<<<blocks_for(n, 256), 256, 0, s>>>(t, n, g, cmap, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_schedule_batch(const RunDesc* runs, int n_runs, int num_sms, cudaStream_t s) {
+    k_cell_schedule_batch<<<num_sms * 4, 256, 0, s>>>(runs, n_runs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_tick_batch(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k, int parity,
+                                   int num_sms, cudaStream_t s) {
+    static int per_sm = 0, configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e =
+            cudaFuncSetAttribute(k_cell_tick_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick_batch, kTickThreads, kTickSmem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        configured_device = dev;
+    }
+    // Persistent over all resident slots; the cell count is read on the device.
+    k_cell_tick_batch<<<per_sm * num_sms, kTickThreads, kTickSmem, s>>>(runs, n_runs, bs, k, parity);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_batch(const RunDesc* runs, int n_runs, cudaStream_t s) {
+    k_compact_batch<<<n_runs, kCompactThreads, 0, s>>>(runs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_changes(const RunDesc* runs, int n_runs, BatchScalars* bs, marl_change* packed,
+                                cudaStream_t s) {
+    k_pack_changes<<<n_runs, 256, 0, s>>>(runs, n_runs, bs, packed);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halve_batch(const RunDesc* runs, const uint2* items, uint32_t count, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_halve_batch<<<blocks_for((size_t)count * MARL_M_INT, 256), 256, 0, s>>>(runs, items, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clear_dead_batch(const RunDesc* runs, const uint2* items, uint32_t count, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_clear_dead_batch<<<blocks_for(count, 256), 256, 0, s>>>(runs, items, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_moves_batch(const RunDesc* runs, const uint4* items, uint32_t count, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_moves_batch<<<blocks_for((size_t)count * 32, 128), 128, 0, s>>>(runs, items, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_births_batch(const RunDesc* runs, const marl_cell* recs, const uint2* slots, uint32_t count,
+                                uint32_t* err, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_births_batch<<<blocks_for(count, 128), 128, 0, s>>>(runs, recs, slots, count, err);
     return cudaGetLastError();
 }
 

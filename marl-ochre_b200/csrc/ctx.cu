@@ -45,7 +45,7 @@ marl_status cuda_fail(cudaError_t e, const char* where) {
         if (_e != cudaSuccess) return cuda_fail(_e, #expr);   \
     } while (0)
 
-static marl_status check_device(int* dev, int* sms) {
+marl_status check_device(int* dev, int* sms) {
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) return fail(MARL_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
@@ -93,7 +93,7 @@ void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck) {
     ck->rush_penalty_rate = p.rush_penalty_rate;
 }
 
-static marl_status validate_dims(int32_t gx, int32_t gy, int32_t gz) {
+marl_status validate_dims(int32_t gx, int32_t gy, int32_t gz) {
     if (gx < 1 || gy < 1 || gz < 1 || gx > kMaxXY || gy > kMaxXY || gz > kMaxZ)
         return fail(MARL_ERR_INVALID_INPUT, "grid %dx%dx%d outside 1..%d x 1..%d x 1..%d", gx, gy, gz, kMaxXY,
                     kMaxXY, kMaxZ);
@@ -105,7 +105,7 @@ static cudaError_t dalloc(T** p, size_t count) {
     return cudaMalloc((void**)p, count * sizeof(T) + 16);
 }
 
-static void free_table(CellTable& t) {
+void free_table(CellTable& t) {
     void* ptrs[] = {t.internal, t.pos, t.age, t.state, t.tp_rate, t.tp_idx, t.rx, t.ef_par, t.ef_idx, t.fate,
                     t.lineage, t.cold, t.nb, t.dep, t.done, t.events};
     for (void* p : ptrs)
@@ -113,7 +113,7 @@ static void free_table(CellTable& t) {
     std::memset(&t, 0, sizeof(t));
 }
 
-static cudaError_t alloc_table(CellTable& t, uint32_t cap) {
+cudaError_t alloc_table(CellTable& t, uint32_t cap) {
     std::memset(&t, 0, sizeof(t));
     t.cap = cap;
     cudaError_t e;

@@ -81,4 +81,11 @@ struct marl_ctx {
 namespace marl {
 marl_status fail(marl_status st, const char* fmt, ...);
 marl_status cuda_fail(cudaError_t e, const char* where);
+// Current device and its SM count; MARL_ERR_NO_DEVICE unless it is sm_100.
+marl_status check_device(int* dev, int* sms);
+marl_status validate_dims(int32_t gx, int32_t gy, int32_t gz);
+void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck);
+// Device cell table of `cap` slots (done[] and events[] zeroed).
+cudaError_t alloc_table(CellTable& t, uint32_t cap);
+void free_table(CellTable& t);
 }  // namespace marl

@@ -12,13 +12,17 @@
 #include <vector>
 
 #include "../../include/marl_cuda.h"
+#include "engine_host.h"
 #include "host_rng.h"
 
 namespace marl {
 marl_status fail(marl_status st, const char* fmt, ...);
 }
+using marl::EditData;
 using marl::fail;
+using marl::HostCell;
 using marl::HostRng;
+using marl::HostRun;
 
 namespace {
 
@@ -164,150 +168,208 @@ void mutate_ruleset(marl_ruleset& rs, HostRng& rng, const marl_sim_params& sim) 
     }
 }
 
-// Host-side cell record kept for fate processing: what the device does not
-// change during a tick (position, lineage, starter type, ruleset).
-struct HostCell {
-    uint16_t pos[3];
-    uint8_t starter_type;
-    uint64_t lineage_id;
-    marl_ruleset ruleset;
-};
-
 }  // namespace
 
-struct marl_engine {
-    marl_ctx* ctx = nullptr;
-    int X = 0, Y = 0, Z = 0;
-    marl_sim_params sim{};
-    HostRng rng;
-    std::vector<HostCell> cells;  // the reference's `cells: Vec<CellState>` order
-    std::vector<int32_t> cmap;    // the reference's `cell_map` as a dense voxel map
-    std::vector<marl_change> changes;
-    uint64_t tick = 0, total_div = 0, total_death = 0, tick_div = 0, tick_death = 0;
-    uint64_t h2d_last = 0, d2h_last = 0;
+namespace marl {
 
-    size_t vox(int x, int y, int z) const { return ((size_t)z * Y + y) * X + x; }
+marl_edit_list EditData::view() const {
+    marl_edit_list e;
+    e.n_halve = (uint32_t)halve.size();
+    e.halve = halve.data();
+    e.n_deaths = (uint32_t)deaths.size();
+    e.deaths = deaths.data();
+    e.n_moves = (uint32_t)move_dst.size();
+    e.move_dst = move_dst.data();
+    e.move_src = move_src.data();
+    e.n_after_deaths = n_after_deaths;
+    e.n_births = (uint32_t)births.size();
+    e.births = births.data();
+    return e;
+}
 
-    // crates/marl-sim/src/spatial.rs:115-154 (find_empty_neighbor)
-    bool find_empty_neighbor(const uint16_t p[3], uint16_t out[3]) {
-        const int dist = (int)sim.division_neighbor_distance;
-        uint16_t cand[6][3];
-        uint32_t nc = 0;
+void HostRun::init(int gx, int gy, int gz, const marl_sim_params& p, uint64_t seed) {
+    X = gx, Y = gy, Z = gz;
+    sim = p;
+    rng.seed_with(seed);
+    cells.clear();
+    cmap.assign((size_t)gx * gy * gz, -1);
+    tick = total_div = total_death = tick_div = tick_death = 0;
+}
+
+marl_status HostRun::seed_default(uint32_t seed_count, std::vector<float>& field, std::vector<marl_cell>& out) {
+    if (X <= 2 * (int)sim.seed_margin || Y <= 2 * (int)sim.seed_margin)
+        return fail(MARL_ERR_INVALID_INPUT, "grid %dx%d too small for seed_margin %u", X, Y, sim.seed_margin);
+    // init_field_boundaries (crates/marl-sim/src/seeding.rs:9-26)
+    field.assign((size_t)X * Y * Z * MARL_S_EXT, 0.0f);
+    const int layers = (int)sim.boundary_prime_layers;
+    for (int y = 0; y < Y; ++y)
+        for (int x = 0; x < X; ++x) {
+            for (int z = 0; z < layers && z < Z; ++z) {
+                field[vox(x, y, z) * 12 + 1] = sim.boundary_prime_oxidant;
+                field[vox(x, y, z) * 12 + 3] = sim.boundary_prime_carbon;
+            }
+            for (int z = std::max(Z - layers, 0); z < Z; ++z) field[vox(x, y, z) * 12 + 2] = sim.boundary_prime_reductant;
+        }
+    // seed_cells x3 with depth bands scaled by Z/200 (lib.rs:59-105, seeding.rs:28-58)
+    out.clear();
+    const float z_scale = (float)Z / 200.0f;
+    const float lo_f[3] = {sim.phototroph_z_lo, sim.chemolithotroph_z_lo, sim.anaerobe_z_lo};
+    const float hi_f[3] = {sim.phototroph_z_hi, sim.chemolithotroph_z_hi, sim.anaerobe_z_hi};
+    const float min_span[3] = {1.0f, 3.0f, 3.0f};
+    for (int kind = 0; kind < 3; ++kind) {
+        const uint16_t lo = (uint16_t)(lo_f[kind] * z_scale);
+        const uint16_t hi = (uint16_t)std::fmax(hi_f[kind] * z_scale, (float)lo + min_span[kind]);
+        const uint32_t zhi = std::min<uint32_t>(hi, (uint32_t)Z);
+        if (seed_count > 0 && lo >= zhi) return fail(MARL_ERR_INVALID_INPUT, "empty seeding depth band [%u,%u)", lo, zhi);
+        uint32_t seeded = 0;
+        for (uint32_t a = 0; a < seed_count * 8 && seeded < seed_count; ++a) {
+            const uint16_t x = (uint16_t)rng.range(sim.seed_margin, (uint32_t)X - sim.seed_margin);
+            const uint16_t y = (uint16_t)rng.range(sim.seed_margin, (uint32_t)Y - sim.seed_margin);
+            const uint16_t z = (uint16_t)rng.range(lo, zhi);
+            const size_t v = vox(x, y, z);
+            if (cmap[v] >= 0) continue;
+            const uint16_t pos[3] = {x, y, z};
+            const marl_cell c = starter(kind, pos, rng.u64());
+            cmap[v] = (int32_t)out.size();
+            out.push_back(c);
+            ++seeded;
+        }
+    }
+    adopt(out.data(), (uint32_t)out.size());
+    return MARL_OK;
+}
+
+void HostRun::adopt(const marl_cell* c, uint32_t n) {
+    cells.clear();
+    std::fill(cmap.begin(), cmap.end(), -1);
+    for (uint32_t i = 0; i < n; ++i) {
+        HostCell h;
+        std::memcpy(h.pos, c[i].pos, sizeof(h.pos));
+        h.starter_type = c[i].starter_type;
+        h.lineage_id = c[i].lineage_id;
+        h.ruleset = c[i].ruleset;
+        cells.push_back(h);
+        cmap[vox(h.pos[0], h.pos[1], h.pos[2])] = (int32_t)i;
+    }
+}
+
+// crates/marl-sim/src/spatial.rs:115-154 (find_empty_neighbor)
+bool HostRun::find_empty_neighbor(const uint16_t p[3], uint16_t out[3]) {
+    const int dist = (int)sim.division_neighbor_distance;
+    uint16_t cand[6][3];
+    uint32_t nc = 0;
+    for (const auto& f : kFace) {
+        const int nx = p[0] + f[0] * dist, ny = p[1] + f[1] * dist, nz = p[2] + f[2] * dist;
+        if (nx >= 0 && nx < X && ny >= 0 && ny < Y && nz >= 0 && nz < Z && cmap[vox(nx, ny, nz)] < 0) {
+            cand[nc][0] = (uint16_t)nx, cand[nc][1] = (uint16_t)ny, cand[nc][2] = (uint16_t)nz;
+            ++nc;
+        }
+    }
+    if (nc == 0) {
         for (const auto& f : kFace) {
-            const int nx = p[0] + f[0] * dist, ny = p[1] + f[1] * dist, nz = p[2] + f[2] * dist;
+            const int nx = p[0] + f[0], ny = p[1] + f[1], nz = p[2] + f[2];
             if (nx >= 0 && nx < X && ny >= 0 && ny < Y && nz >= 0 && nz < Z && cmap[vox(nx, ny, nz)] < 0) {
                 cand[nc][0] = (uint16_t)nx, cand[nc][1] = (uint16_t)ny, cand[nc][2] = (uint16_t)nz;
                 ++nc;
             }
         }
-        if (nc == 0) {
-            for (const auto& f : kFace) {
-                const int nx = p[0] + f[0], ny = p[1] + f[1], nz = p[2] + f[2];
-                if (nx >= 0 && nx < X && ny >= 0 && ny < Y && nz >= 0 && nz < Z && cmap[vox(nx, ny, nz)] < 0) {
-                    cand[nc][0] = (uint16_t)nx, cand[nc][1] = (uint16_t)ny, cand[nc][2] = (uint16_t)nz;
-                    ++nc;
-                }
-            }
-            if (nc == 0) return false;
-        }
-        const uint32_t i = rng.range(0, nc);
-        std::memcpy(out, cand[i], sizeof(uint16_t) * 3);
-        return true;
+        if (nc == 0) return false;
     }
+    const uint32_t i = rng.range(0, nc);
+    std::memcpy(out, cand[i], sizeof(uint16_t) * 3);
+    return true;
+}
 
-    // crates/marl-sim/src/lib.rs:219-277 (fate processing) -> edit list
-    marl_status process_changes(uint32_t count) {
-        tick_div = tick_death = 0;
-        std::vector<marl_cell> births;
-        std::vector<uint32_t> halve, deaths;
-        for (uint32_t k = 0; k < count; ++k) {
-            const marl_change& ch = changes[k];
-            if (ch.cell >= cells.size()) return fail(MARL_ERR_STATE, "change list names cell %u of %zu", ch.cell,
-                                                     cells.size());
-            if (ch.event == MARL_EVENT_DIVISION) {
-                const HostCell& parent = cells[ch.cell];
-                uint16_t dpos[3];
-                if (find_empty_neighbor(parent.pos, dpos)) {
-                    marl_cell d;
-                    std::memset(&d, 0, sizeof(d));
-                    std::memcpy(d.pos, dpos, sizeof(dpos));
-                    d.quiescent = ch.quiescent;
-                    d.starter_type = parent.starter_type;
-                    d.age = 0;
-                    d.prep_remaining = 0;
-                    d.lineage_id = rng.u64();
-                    for (int i = 0; i < MARL_M_INT; ++i) d.internal[i] = ch.internal[i] * 0.5f;
-                    d.ruleset = parent.ruleset;
-                    halve.push_back(ch.cell);
-                    mutate_ruleset(d.ruleset, rng, sim);
-                    births.push_back(d);
-                    ++tick_div;
-                }
-            } else if (ch.event == MARL_EVENT_DEATH) {
-                deaths.push_back(ch.cell);
-                ++tick_death;
+// crates/marl-sim/src/lib.rs:219-277 (fate processing) -> edit list
+marl_status HostRun::process(const marl_change* changes, uint32_t count, EditData& e) {
+    tick_div = tick_death = 0;
+    e.halve.clear(), e.deaths.clear(), e.move_dst.clear(), e.move_src.clear(), e.births.clear();
+    std::vector<marl_cell> births;
+    for (uint32_t k = 0; k < count; ++k) {
+        const marl_change& ch = changes[k];
+        if (ch.cell >= cells.size())
+            return fail(MARL_ERR_STATE, "change list names cell %u of %zu", ch.cell, cells.size());
+        if (ch.event == MARL_EVENT_DIVISION) {
+            const HostCell& parent = cells[ch.cell];
+            uint16_t dpos[3];
+            if (find_empty_neighbor(parent.pos, dpos)) {
+                marl_cell d;
+                std::memset(&d, 0, sizeof(d));
+                std::memcpy(d.pos, dpos, sizeof(dpos));
+                d.quiescent = ch.quiescent;
+                d.starter_type = parent.starter_type;
+                d.age = 0;
+                d.prep_remaining = 0;
+                d.lineage_id = rng.u64();
+                for (int i = 0; i < MARL_M_INT; ++i) d.internal[i] = ch.internal[i] * 0.5f;
+                d.ruleset = parent.ruleset;
+                e.halve.push_back(ch.cell);
+                mutate_ruleset(d.ruleset, rng, sim);
+                births.push_back(d);
+                ++tick_div;
             }
+        } else if (ch.event == MARL_EVENT_DEATH) {
+            e.deaths.push_back(ch.cell);
+            ++tick_death;
         }
-        total_div += tick_div;
-        total_death += tick_death;
-        // Deaths arrive in ascending cell order without duplicates (one event
-        // per cell); remove them back to front with swap_remove, tracking
-        // which original slot ends up in each hole.
-        const uint32_t n0 = (uint32_t)cells.size();
-        std::vector<uint32_t> origin(n0);
-        for (uint32_t i = 0; i < n0; ++i) origin[i] = i;
-        for (auto it = deaths.rbegin(); it != deaths.rend(); ++it) {
-            const uint32_t i = *it;
-            cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = -1;
-            cells[i] = cells.back();
-            origin[i] = origin[cells.size() - 1];
-            cells.pop_back();
-            if (i < cells.size()) cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = (int32_t)i;
-        }
-        const uint32_t n_after = (uint32_t)cells.size();
-        std::vector<uint32_t> mdst, msrc;
-        for (uint32_t d : deaths)
-            if (d < n_after && origin[d] != d) {
-                mdst.push_back(d);
-                msrc.push_back(origin[d]);
-            }
-        // Births append unless the voxel was taken meanwhile (lib.rs:270-277).
-        std::vector<marl_cell> accepted;
-        for (auto& b : births) {
-            const size_t v = vox(b.pos[0], b.pos[1], b.pos[2]);
-            if (cmap[v] < 0) {
-                cmap[v] = (int32_t)cells.size();
-                HostCell h;
-                std::memcpy(h.pos, b.pos, sizeof(h.pos));
-                h.starter_type = b.starter_type;
-                h.lineage_id = b.lineage_id;
-                h.ruleset = b.ruleset;
-                cells.push_back(h);
-                accepted.push_back(b);
-            }
-        }
-        marl_edit_list e;
-        e.n_halve = (uint32_t)halve.size();
-        e.halve = halve.data();
-        e.n_deaths = (uint32_t)deaths.size();
-        e.deaths = deaths.data();
-        e.n_moves = (uint32_t)mdst.size();
-        e.move_dst = mdst.data();
-        e.move_src = msrc.data();
-        e.n_after_deaths = n_after;
-        e.n_births = (uint32_t)accepted.size();
-        e.births = accepted.data();
-        return marl_apply_edits(ctx, &e);
     }
+    total_div += tick_div;
+    total_death += tick_death;
+    // Deaths arrive in ascending cell order without duplicates (one event per
+    // cell); remove them back to front with swap_remove, tracking which
+    // original slot ends up in each hole.
+    const uint32_t n0 = (uint32_t)cells.size();
+    std::vector<uint32_t> origin(n0);
+    for (uint32_t i = 0; i < n0; ++i) origin[i] = i;
+    for (auto it = e.deaths.rbegin(); it != e.deaths.rend(); ++it) {
+        const uint32_t i = *it;
+        cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = -1;
+        cells[i] = cells.back();
+        origin[i] = origin[cells.size() - 1];
+        cells.pop_back();
+        if (i < cells.size()) cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = (int32_t)i;
+    }
+    e.n_after_deaths = (uint32_t)cells.size();
+    for (uint32_t d : e.deaths)
+        if (d < e.n_after_deaths && origin[d] != d) {
+            e.move_dst.push_back(d);
+            e.move_src.push_back(origin[d]);
+        }
+    // Births append unless the voxel was taken meanwhile (lib.rs:270-277).
+    for (auto& b : births) {
+        const size_t v = vox(b.pos[0], b.pos[1], b.pos[2]);
+        if (cmap[v] < 0) {
+            cmap[v] = (int32_t)cells.size();
+            HostCell h;
+            std::memcpy(h.pos, b.pos, sizeof(h.pos));
+            h.starter_type = b.starter_type;
+            h.lineage_id = b.lineage_id;
+            h.ruleset = b.ruleset;
+            cells.push_back(h);
+            e.births.push_back(b);
+        }
+    }
+    ++tick;
+    return MARL_OK;
+}
+
+}  // namespace marl
+
+struct marl_engine {
+    marl_ctx* ctx = nullptr;
+    HostRun run;
+    EditData edits;
+    std::vector<marl_change> changes;
+    uint64_t h2d_last = 0, d2h_last = 0;
 
     marl_status step_once() {
         uint32_t count = 0;
-        if (changes.size() < cells.size() + 1) changes.resize(cells.size() + 1);
+        if (changes.size() < run.cells.size() + 1) changes.resize(run.cells.size() + 1);
         marl_status st = marl_tick(ctx, changes.data(), (uint32_t)changes.size(), &count);
         if (st) return st;
-        if ((st = process_changes(count))) return st;
-        ++tick;
-        return MARL_OK;
+        if ((st = run.process(changes.data(), count, edits))) return st;
+        const marl_edit_list e = edits.view();
+        return marl_apply_edits(ctx, &e);
     }
 };
 
@@ -317,86 +379,22 @@ extern "C" {
 uint64_t marl_internal_ctx_h2d(marl_ctx* c);
 uint64_t marl_internal_ctx_d2h(marl_ctx* c);
 
-static marl_status engine_init(marl_engine* e, int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim,
-                               uint64_t seed, uint32_t cap) {
-    e->X = gx, e->Y = gy, e->Z = gz;
-    e->sim = *sim;
-    e->rng.seed_with(seed);
-    e->cmap.assign((size_t)gx * gy * gz, -1);
-    return marl_ctx_create(gx, gy, gz, sim, cap, &e->ctx);
-}
-
-static marl_status engine_upload(marl_engine* e, const std::vector<float>& field, const std::vector<marl_cell>& cells) {
-    marl_status st = marl_upload_field(e->ctx, field.data());
-    if (st) return st;
-    return marl_upload_cells(e->ctx, cells.data(), (uint32_t)cells.size());
-}
-
 marl_status marl_engine_create(int32_t gx, int32_t gy, int32_t gz, const marl_sim_params* sim, uint64_t rng_seed,
                                uint32_t seed_count, uint32_t cell_capacity, marl_engine** out) {
     if (!sim || !out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     *out = nullptr;
-    if (gx <= 2 * (int)sim->seed_margin || gy <= 2 * (int)sim->seed_margin)
-        return fail(MARL_ERR_INVALID_INPUT, "grid %dx%d too small for seed_margin %u", gx, gy, sim->seed_margin);
     marl_engine* e = new (std::nothrow) marl_engine();
     if (!e) return fail(MARL_ERR_OUT_OF_MEMORY, "host allocation");
-    marl_status st = engine_init(e, gx, gy, gz, sim, rng_seed, cell_capacity);
-    if (st) {
-        delete e;
-        return st;
-    }
-    // init_field_boundaries (crates/marl-sim/src/seeding.rs:9-26)
-    std::vector<float> field((size_t)gx * gy * gz * MARL_S_EXT, 0.0f);
-    const int layers = (int)sim->boundary_prime_layers;
-    for (int y = 0; y < gy; ++y)
-        for (int x = 0; x < gx; ++x) {
-            for (int z = 0; z < layers && z < gz; ++z) {
-                field[e->vox(x, y, z) * 12 + 1] = sim->boundary_prime_oxidant;
-                field[e->vox(x, y, z) * 12 + 3] = sim->boundary_prime_carbon;
-            }
-            for (int z = std::max(gz - layers, 0); z < gz; ++z) field[e->vox(x, y, z) * 12 + 2] = sim->boundary_prime_reductant;
-        }
-    // seed_cells x3 with depth bands scaled by Z/200 (lib.rs:59-105, seeding.rs:28-58)
+    e->run.init(gx, gy, gz, *sim, rng_seed);
+    std::vector<float> field;
     std::vector<marl_cell> cells;
-    const float z_scale = (float)gz / 200.0f;
-    const float lo_f[3] = {sim->phototroph_z_lo, sim->chemolithotroph_z_lo, sim->anaerobe_z_lo};
-    const float hi_f[3] = {sim->phototroph_z_hi, sim->chemolithotroph_z_hi, sim->anaerobe_z_hi};
-    const float min_span[3] = {1.0f, 3.0f, 3.0f};
-    for (int kind = 0; kind < 3; ++kind) {
-        const uint16_t lo = (uint16_t)(lo_f[kind] * z_scale);
-        const uint16_t hi = (uint16_t)std::fmax(hi_f[kind] * z_scale, (float)lo + min_span[kind]);
-        const uint32_t zhi = std::min<uint32_t>(hi, (uint32_t)gz);
-        if (seed_count > 0 && lo >= zhi) {
-            marl_engine_destroy(e);
-            return fail(MARL_ERR_INVALID_INPUT, "empty seeding depth band [%u,%u)", lo, zhi);
-        }
-        uint32_t seeded = 0;
-        for (uint32_t a = 0; a < seed_count * 8 && seeded < seed_count; ++a) {
-            const uint16_t x = (uint16_t)e->rng.range(sim->seed_margin, (uint32_t)gx - sim->seed_margin);
-            const uint16_t y = (uint16_t)e->rng.range(sim->seed_margin, (uint32_t)gy - sim->seed_margin);
-            const uint16_t z = (uint16_t)e->rng.range(lo, zhi);
-            const size_t v = e->vox(x, y, z);
-            if (e->cmap[v] >= 0) continue;
-            const uint16_t pos[3] = {x, y, z};
-            const marl_cell c = starter(kind, pos, e->rng.u64());
-            e->cmap[v] = (int32_t)cells.size();
-            cells.push_back(c);
-            ++seeded;
-        }
-    }
-    if (cells.size() > cell_capacity) {
-        marl_engine_destroy(e);
-        return fail(MARL_ERR_CAPACITY, "%zu seeded cells exceed capacity %u", cells.size(), cell_capacity);
-    }
-    for (const auto& c : cells) {
-        HostCell h;
-        std::memcpy(h.pos, c.pos, sizeof(h.pos));
-        h.starter_type = c.starter_type;
-        h.lineage_id = c.lineage_id;
-        h.ruleset = c.ruleset;
-        e->cells.push_back(h);
-    }
-    if ((st = engine_upload(e, field, cells))) {
+    marl_status st = e->run.seed_default(seed_count, field, cells);
+    if (!st && cells.size() > cell_capacity)
+        st = fail(MARL_ERR_CAPACITY, "%zu seeded cells exceed capacity %u", cells.size(), cell_capacity);
+    if (!st) st = marl_ctx_create(gx, gy, gz, sim, cell_capacity, &e->ctx);
+    if (!st) st = marl_upload_field(e->ctx, field.data());
+    if (!st) st = marl_upload_cells(e->ctx, cells.data(), (uint32_t)cells.size());
+    if (st) {
         marl_engine_destroy(e);
         return st;
     }
@@ -411,26 +409,15 @@ marl_status marl_engine_create_from_state(int32_t gx, int32_t gy, int32_t gz, co
     *out = nullptr;
     marl_engine* e = new (std::nothrow) marl_engine();
     if (!e) return fail(MARL_ERR_OUT_OF_MEMORY, "host allocation");
-    marl_status st = engine_init(e, gx, gy, gz, sim, rng_seed, cell_capacity);
+    marl_status st = marl_ctx_create(gx, gy, gz, sim, cell_capacity, &e->ctx);
+    if (!st) st = marl_upload_field(e->ctx, field);
+    if (!st) st = marl_upload_cells(e->ctx, cells, n);  // validates positions
     if (st) {
-        delete e;
-        return st;
-    }
-    std::vector<float> f(field, field + (size_t)gx * gy * gz * MARL_S_EXT);
-    std::vector<marl_cell> cv(cells, cells + n);
-    if ((st = engine_upload(e, f, cv))) {  // validates positions
         marl_engine_destroy(e);
         return st;
     }
-    for (uint32_t i = 0; i < n; ++i) {
-        HostCell h;
-        std::memcpy(h.pos, cells[i].pos, sizeof(h.pos));
-        h.starter_type = cells[i].starter_type;
-        h.lineage_id = cells[i].lineage_id;
-        h.ruleset = cells[i].ruleset;
-        e->cells.push_back(h);
-        e->cmap[e->vox(h.pos[0], h.pos[1], h.pos[2])] = (int32_t)i;
-    }
+    e->run.init(gx, gy, gz, *sim, rng_seed);
+    e->run.adopt(cells, n);
     *out = e;
     return MARL_OK;
 }
@@ -460,12 +447,12 @@ marl_status marl_engine_step(marl_engine* e, uint32_t ticks) {
 
 marl_status marl_engine_stats_get(marl_engine* e, marl_engine_stats* s) {
     if (!e || !s) return fail(MARL_ERR_INVALID_INPUT, "null argument");
-    s->tick = e->tick;
-    s->population = e->cells.size();
-    s->total_divisions = e->total_div;
-    s->total_deaths = e->total_death;
-    s->tick_divisions = e->tick_div;
-    s->tick_deaths = e->tick_death;
+    s->tick = e->run.tick;
+    s->population = e->run.cells.size();
+    s->total_divisions = e->run.total_div;
+    s->total_deaths = e->run.total_death;
+    s->tick_divisions = e->run.tick_div;
+    s->tick_deaths = e->run.tick_death;
     s->h2d_bytes_last_tick = e->h2d_last;
     s->d2h_bytes_last_tick = e->d2h_last;
     return MARL_OK;

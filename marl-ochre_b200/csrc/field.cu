@@ -201,11 +201,10 @@ __device__ __forceinline__ void stencil(float out[12], const Vox& c, const Vox& 
 // on them.  Results go to a triple-buffered shared tile; one TMA bulk-tensor
 // store per plane writes it back.  One barrier per plane.
 template <int TY, int STAGES>
-__global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__ CUtensorMap tm_src,
-                                                        const __grid_constant__ CUtensorMap tm_dst,
-                                                        const __grid_constant__ CUtensorMap tm_mask, Grid g, int zc,
-                                                        FieldConsts k, int apply_sources, float* __restrict__ c4_out,
-                                                        uint32_t* __restrict__ err) {
+__device__ __forceinline__ void diffuse_tile(const CUtensorMap* tm_src, const CUtensorMap* tm_dst,
+                                             const CUtensorMap* tm_mask, const Grid g, const int bx, const int by,
+                                             const int bz, const int zc, const FieldConsts& k, const int apply_sources,
+                                             float* __restrict__ c4_out, uint32_t* __restrict__ err) {
     using T = DiffTile<TY, STAGES>;
     constexpr int TX = T::TX;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -218,7 +217,7 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * zc;
+    const int x0 = bx * TX, y0 = by * TY, z0 = bz * zc;
     const int z1 = min(z0 + zc, g.Z);
     const int nplanes = z1 - z0 + 2;  // planes z0-1 .. z1
     const int last = nplanes - 2;     // centre planes 1 .. last
@@ -236,8 +235,8 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
         // Planes outside the grid are never read (walls use the centre
         // value), so they are loaded from a clamped in-grid z.
         const int zz = min(max(z0 - 1 + p, 0), g.Z - 1);
-        tma_load_3d(plane_of(p), &tm_src, (x0 - 1) * 12, y0 - 1, zz, bar);
-        tma_load_3d((void*)mask_of(p), &tm_mask, x0 - 16, y0 - 1, zz, bar);
+        tma_load_3d(plane_of(p), tm_src, (x0 - 1) * 12, y0 - 1, zz, bar);
+        tma_load_3d((void*)mask_of(p), tm_mask, x0 - 16, y0 - 1, zz, bar);
     };
     auto is_source_plane = [&](int p) {
         const int z = z0 - 1 + p;
@@ -354,7 +353,7 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
             return false;
         }
         if (tid == 0) {
-            tma_store_3d(&tm_dst, outbuf + (p % 3) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
+            tma_store_3d(tm_dst, outbuf + (p % 3) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
             bulk_commit();
             bulk_wait_read<1>();  // the store of plane p-1 has read its buffer
         }
@@ -381,6 +380,32 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
     }
 }
 
+template <int TY, int STAGES>
+__global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__ CUtensorMap tm_src,
+                                                        const __grid_constant__ CUtensorMap tm_dst,
+                                                        const __grid_constant__ CUtensorMap tm_mask, Grid g, int zc,
+                                                        FieldConsts k, int apply_sources, float* __restrict__ c4_out,
+                                                        uint32_t* __restrict__ err) {
+    diffuse_tile<TY, STAGES>(&tm_src, &tm_dst, &tm_mask, g, blockIdx.x, blockIdx.y, blockIdx.z, zc, k, apply_sources,
+                             c4_out, err);
+}
+
+// Batched form: one launch advances one substep of every run.  CTA b owns
+// work item items[b] = (run, tile x, tile y, z-chunk); the run's tensor maps
+// (loads from buffer 0/1, stores into buffer 0/1, mask) are read from global
+// memory.  All runs share the ping-pong parity of the substep.
+template <int TY, int STAGES>
+__global__ void __launch_bounds__(kDiffTX* TY)
+    k_diffuse_batch(const RunDesc* __restrict__ runs, const CUtensorMap* __restrict__ maps,
+                    const int4* __restrict__ items, int zc, FieldConsts k, int parity, int apply_sources, int emit_c4,
+                    uint32_t* __restrict__ err) {
+    const int4 it = items[blockIdx.x];
+    const RunDesc& r = runs[it.x];
+    const CUtensorMap* m = maps + (size_t)it.x * kMapsPerRun;
+    diffuse_tile<TY, STAGES>(&m[parity], &m[2 + (parity ^ 1)], &m[4], r.g, it.y, it.z, it.w, zc, k, apply_sources,
+                             emit_c4 ? r.c4 : nullptr, err);
+}
+
 // ------------------------------------------------------------ light ------
 // crates/marl-field/src/light.rs:29-59.  The running intensity of a column is
 // an exclusive product with a floor to zero; the floor makes it
@@ -392,12 +417,11 @@ __global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__
 constexpr int kLightCols = 32;
 constexpr int kLightSeg = 64;
 
-__global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, const float* __restrict__ field,
-                                               const uint8_t* __restrict__ mask, float* __restrict__ light, Grid g,
-                                               FieldConsts k) {
+__device__ __forceinline__ void light_columns(const float* __restrict__ c4, const float* __restrict__ field,
+                                              const uint8_t* __restrict__ mask, float* __restrict__ light,
+                                              const Grid g, const FieldConsts& k, const int x0, const int y) {
     __shared__ float fac[kLightSeg][kLightCols];
     __shared__ uint8_t occ[kLightSeg][kLightCols];
-    const int x0 = blockIdx.x * kLightCols, y = blockIdx.y;
     const int tid = threadIdx.x, lane = tid & 31;
     const int pitch = mask_pitch(g.X);
     const float neg_chem = -k.chemical_absorption;
@@ -426,6 +450,22 @@ __global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, con
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, const float* __restrict__ field,
+                                               const uint8_t* __restrict__ mask, float* __restrict__ light, Grid g,
+                                               FieldConsts k) {
+    light_columns(c4, field, mask, light, g, k, blockIdx.x * kLightCols, blockIdx.y);
+}
+
+// Batched form: block b handles item (run, column chunk, y) of any run.
+// With use_c4 species 4 comes from the run's compact copy written by the
+// last substep, otherwise from field[parity].
+__global__ void __launch_bounds__(256) k_light_batch(const RunDesc* __restrict__ runs, const int4* __restrict__ items,
+                                                     FieldConsts k, int parity, int use_c4) {
+    const int4 it = items[blockIdx.x];
+    const RunDesc& r = runs[it.x];
+    light_columns(use_c4 ? r.c4 : nullptr, r.field[parity], r.mask, r.light, r.g, k, it.y * kLightCols, it.z);
 }
 
 // ------------------------------------------------------------- mass ------
@@ -540,6 +580,48 @@ cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const Grid&
         case 6: return launch_diffuse_t<4, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
         default: return launch_diffuse_t<32, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
     }
+}
+
+template <int TY, int STAGES>
+static cudaError_t launch_diffuse_batch_t(const RunDesc* runs, const CUtensorMap* maps, const int4* items, int n_items,
+                                          int zc, const FieldConsts& k, int parity, int apply_sources, int emit_c4,
+                                          uint32_t* err, cudaStream_t s) {
+    using T = DiffTile<TY, STAGES>;
+    if (n_items == 0) return cudaSuccess;
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e = cudaFuncSetAttribute(k_diffuse_batch<TY, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             T::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    k_diffuse_batch<TY, STAGES><<<n_items, kDiffTX * TY, T::SMEM_BYTES, s>>>(runs, maps, items, zc, k, parity,
+                                                                           apply_sources, emit_c4, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diffuse_batch(int tile, const RunDesc* runs, const CUtensorMap* maps, const int4* items,
+                                 int n_items, int zc, const FieldConsts& k, int parity, int apply_sources, int emit_c4,
+                                 uint32_t* err, cudaStream_t s) {
+    switch (tile) {
+        case 0: return launch_diffuse_batch_t<8, 4>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 1: return launch_diffuse_batch_t<16, 4>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 2: return launch_diffuse_batch_t<4, 4>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 3: return launch_diffuse_batch_t<32, 4>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 4: return launch_diffuse_batch_t<8, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 5: return launch_diffuse_batch_t<16, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 6: return launch_diffuse_batch_t<4, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        default: return launch_diffuse_batch_t<32, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+    }
+}
+
+cudaError_t launch_light_batch(const RunDesc* runs, const int4* items, int n_items, const FieldConsts& k, int parity,
+                               int use_c4, cudaStream_t s) {
+    if (n_items == 0) return cudaSuccess;
+    k_light_batch<<<n_items, 256, 0, s>>>(runs, items, k, parity, use_c4);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_sources(float* f, const Grid& g, const FieldConsts& k, cudaStream_t s) {

@@ -50,6 +50,60 @@ struct ChangeHeader {  // device-written, read back with the change list
 };
 static_assert(sizeof(ChangeHeader) == 64, "change header is 64 bytes");
 
+// One run of a batch, as the batched kernels see it (device memory).
+struct RunDesc {
+    Grid g;
+    uint32_t n;          // cells
+    uint32_t epoch;      // this tick's completion epoch
+    uint32_t cell_base;  // global ticket of this run's cell 0
+    uint32_t pad;
+    float* field[2];
+    uint8_t* mask;
+    int32_t* cmap;
+    float* light;
+    float* c4;
+    CellTable t;
+    ChangeHeader* hdr;
+    marl_change* changes;
+    uint32_t change_cap;
+    uint32_t pad2;
+};
+// Tensor maps per run in the batch's map array: load from buffer 0 / 1,
+// store into buffer 0 / 1, occupancy mask.
+constexpr int kMapsPerRun = 5;
+
+// Batch-wide scalars in device memory.  The cell total of the batch is not
+// stored: it is cell_base + n of the last run.
+struct BatchScalars {
+    uint32_t ticket;   // cell-tick ticket counter (zeroed before each tick)
+    uint32_t err;      // kErr* bits of every batched kernel
+    uint32_t changes;  // Division/Death events over all runs (set by the pack kernel)
+    uint32_t pad[13];
+};
+static_assert(sizeof(BatchScalars) == 64, "batch scalars are 64 bytes");
+
+// Batched launchers (one launch covers every run).
+cudaError_t launch_diffuse_batch(int tile, const RunDesc* runs, const CUtensorMap* maps, const int4* items,
+                                 int n_items, int zc, const FieldConsts& k, int parity, int apply_sources, int emit_c4,
+                                 uint32_t* err, cudaStream_t s);
+cudaError_t launch_light_batch(const RunDesc* runs, const int4* items, int n_items, const FieldConsts& k, int parity,
+                               int use_c4, cudaStream_t s);
+cudaError_t launch_cell_schedule_batch(const RunDesc* runs, int n_runs, int num_sms, cudaStream_t s);
+cudaError_t launch_cell_tick_batch(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k, int parity,
+                                   int num_sms, cudaStream_t s);
+cudaError_t launch_compact_batch(const RunDesc* runs, int n_runs, cudaStream_t s);
+// Concatenates the runs' change lists in run order into `packed` (run r's
+// entries start at the sum of the counts of runs < r) and stores the total
+// in bs->changes.
+cudaError_t launch_pack_changes(const RunDesc* runs, int n_runs, BatchScalars* bs, marl_change* packed,
+                                cudaStream_t s);
+// Edit items: (run, index) pairs, (run, dst, src) moves, (run, slot) births.
+cudaError_t launch_halve_batch(const RunDesc* runs, const uint2* items, uint32_t count, cudaStream_t s);
+cudaError_t launch_clear_dead_batch(const RunDesc* runs, const uint2* items, uint32_t count, cudaStream_t s);
+cudaError_t launch_moves_batch(const RunDesc* runs, const uint4* items, uint32_t count, cudaStream_t s);
+cudaError_t launch_births_batch(const RunDesc* runs, const marl_cell* recs, const uint2* slots, uint32_t count,
+                                uint32_t* err, cudaStream_t s);
+
 struct CellLaunch {
     CellTable t;
     uint32_t n;

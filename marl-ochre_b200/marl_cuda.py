@@ -120,6 +120,11 @@ class EditList(ctypes.Structure):
     ]
 
 
+class RunSpec(ctypes.Structure):
+    _fields_ = [("gx", c_int32), ("gy", c_int32), ("gz", c_int32), ("seed_count", c_uint32), ("rng_seed", c_uint64),
+                ("cell_capacity", c_uint32), ("_pad", c_uint32)]
+
+
 class MarlError(RuntimeError):
     def __init__(self, status: int, where: str, message: str = ""):
         self.status = status
@@ -144,6 +149,10 @@ EXPORTED = [
     "marl_engine_create", "marl_engine_create_from_state", "marl_engine_destroy", "marl_engine_set_stream",
     "marl_engine_step", "marl_engine_stats_get", "marl_engine_get_cells", "marl_engine_get_field",
     "marl_engine_get_light", "marl_engine_ctx",
+    "marl_batch_create", "marl_batch_destroy", "marl_batch_set_stream", "marl_batch_set_host_threads",
+    "marl_batch_set_tile", "marl_batch_get_tile", "marl_batch_autotune", "marl_batch_set_graph", "marl_batch_step",
+    "marl_batch_run_count", "marl_batch_stats_get", "marl_batch_get_cells", "marl_batch_get_field",
+    "marl_batch_get_light", "marl_batch_counters",
 ]
 
 _lib = None
@@ -203,6 +212,21 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_engine_get_field": (c_int32, [P, P]),
         "marl_engine_get_light": (c_int32, [P, P]),
         "marl_engine_ctx": (c_void_p, [P]),
+        "marl_batch_create": (c_int32, [POINTER(RunSpec), c_uint32, POINTER(SimParams), POINTER(c_void_p)]),
+        "marl_batch_destroy": (None, [P]),
+        "marl_batch_set_stream": (c_int32, [P, P]),
+        "marl_batch_set_host_threads": (c_int32, [P, c_int32]),
+        "marl_batch_set_tile": (c_int32, [P, c_int32, c_int32]),
+        "marl_batch_get_tile": (c_int32, [P, POINTER(c_int32), POINTER(c_int32)]),
+        "marl_batch_autotune": (c_int32, [P, c_int32, POINTER(c_float)]),
+        "marl_batch_set_graph": (c_int32, [P, c_int32]),
+        "marl_batch_step": (c_int32, [P, c_uint32]),
+        "marl_batch_run_count": (c_int32, [P, POINTER(c_uint32)]),
+        "marl_batch_stats_get": (c_int32, [P, c_uint32, POINTER(EngineStats)]),
+        "marl_batch_get_cells": (c_int32, [P, c_uint32, P, c_uint32, POINTER(c_uint32)]),
+        "marl_batch_get_field": (c_int32, [P, c_uint32, P]),
+        "marl_batch_get_light": (c_int32, [P, c_uint32, P]),
+        "marl_batch_counters": (c_int32, [P, POINTER(Counters)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -518,4 +542,98 @@ class Engine:
         X, Y, Z = self.dims
         out = np.empty((Z, Y, X), np.float32)
         _check(self.lib.marl_engine_get_light(self.h, _ptr(out)), "marl_engine_get_light")
+        return out
+
+
+class Batch:
+    """Many independent runs advanced together — marl_batch.
+
+    `runs` is a list of (dims, rng_seed) or (dims, rng_seed, seed_count,
+    cell_capacity); run r behaves exactly like Engine(dims, params, rng_seed,
+    seed_count, cell_capacity)."""
+
+    def __init__(self, runs, params: SimParams | None = None, seed_count: int = 30, cell_capacity: int = 0):
+        self.lib = load()
+        self.params = (params or default_params()).copy()
+        specs = (RunSpec * len(runs))()
+        self.dims = []
+        for i, r in enumerate(runs):
+            dims, seed = r[0], r[1]
+            sc = r[2] if len(r) > 2 else seed_count
+            cap = r[3] if len(r) > 3 else cell_capacity
+            X, Y, Z = (int(d) for d in dims)
+            specs[i] = RunSpec(X, Y, Z, sc, seed, cap, 0)
+            self.dims.append((X, Y, Z))
+        h = c_void_p()
+        _check(self.lib.marl_batch_create(specs, len(runs), ctypes.byref(self.params), ctypes.byref(h)),
+               "marl_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.marl_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self.dims)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib.marl_batch_set_stream(self.h, c_void_p(stream_ptr)), "marl_batch_set_stream")
+
+    def set_host_threads(self, threads: int) -> None:
+        _check(self.lib.marl_batch_set_host_threads(self.h, threads), "marl_batch_set_host_threads")
+
+    def set_tile(self, tile: int, zc: int) -> None:
+        _check(self.lib.marl_batch_set_tile(self.h, tile, zc), "marl_batch_set_tile")
+
+    def get_tile(self) -> tuple[int, int]:
+        t, z = c_int32(), c_int32()
+        _check(self.lib.marl_batch_get_tile(self.h, ctypes.byref(t), ctypes.byref(z)), "marl_batch_get_tile")
+        return t.value, z.value
+
+    def autotune(self, reps: int = 5) -> float:
+        us = c_float()
+        _check(self.lib.marl_batch_autotune(self.h, reps, ctypes.byref(us)), "marl_batch_autotune")
+        return us.value
+
+    def set_graph(self, use_graph: bool) -> None:
+        _check(self.lib.marl_batch_set_graph(self.h, 1 if use_graph else 0), "marl_batch_set_graph")
+
+    def step(self, ticks: int = 1) -> None:
+        _check(self.lib.marl_batch_step(self.h, ticks), "marl_batch_step")
+
+    def counters(self) -> dict:
+        c = Counters()
+        _check(self.lib.marl_batch_counters(self.h, ctypes.byref(c)), "marl_batch_counters")
+        return {name: getattr(c, name) for name, _ in Counters._fields_}
+
+    def stats(self, run: int) -> dict:
+        s = EngineStats()
+        _check(self.lib.marl_batch_stats_get(self.h, run, ctypes.byref(s)), "marl_batch_stats_get")
+        return {name: getattr(s, name) for name, _ in EngineStats._fields_}
+
+    def cells(self, run: int) -> np.ndarray:
+        n = self.stats(run)["population"]
+        out = np.zeros(max(int(n), 1), CELL_DTYPE)
+        got = c_uint32()
+        _check(self.lib.marl_batch_get_cells(self.h, run, _ptr(out), out.size, ctypes.byref(got)),
+               "marl_batch_get_cells")
+        return out[: got.value]
+
+    def field(self, run: int) -> np.ndarray:
+        X, Y, Z = self.dims[run]
+        out = np.empty((Z, Y, X, S_EXT), np.float32)
+        _check(self.lib.marl_batch_get_field(self.h, run, _ptr(out)), "marl_batch_get_field")
+        return out
+
+    def light(self, run: int) -> np.ndarray:
+        X, Y, Z = self.dims[run]
+        out = np.empty((Z, Y, X), np.float32)
+        _check(self.lib.marl_batch_get_light(self.h, run, _ptr(out)), "marl_batch_get_light")
         return out
