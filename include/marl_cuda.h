@@ -408,6 +408,105 @@ marl_status marl_batch_get_light(marl_batch* b, uint32_t run, float* light);
 /* As marl_ctx_counters, over the whole batch (ticks counts batch ticks). */
 marl_status marl_batch_counters(marl_batch* b, marl_counters* out);
 
+/* ---- learned reaction surrogate ----------------------------------------
+ * No counterpart in the reference.  A 93 -> 256 -> 256 -> 16 MLP (tanh-form
+ * GELU, BF16 weights and activations, FP32 accumulation on the tcgen05 tensor
+ * cores) that stands in for the reaction phase of CellState::tick
+ * (crates/marl-cell/src/cell.rs:246-285).  Input features, per cell:
+ *   [0,16)   internal species after transport, light in slot 15 (cell.rs:243)
+ *   [16,28)  gathered neighbour environment (spatial.rs:56-77)
+ *   [28]     light at the cell's voxel
+ *   [29,93)  per reaction r: k_m, v_max, k_cat, cofactor flag (1 = has one)
+ * Output: the 16 internal-species deltas of the reaction phase.  k_m, |v_max|
+ * and k_cat enter as log(v + 1e-3); every feature and target is standardised
+ * with statistics of the training set.
+ *
+ * Training pairs come from the plain cell kernel itself: a context in capture
+ * mode appends one raw row per updated cell and tick (features, then the
+ * plain kernel's deltas).  Training runs forward, backward and Adam on the
+ * GPU.  In a tick, the gated mode predicts every cell's deltas from a
+ * pre-pass over the tick's starting field; a cell whose post-transport state
+ * equals the pre-pass state takes the prediction when it agrees with the
+ * plain reaction phase within `tol` (normwise: max |x_mlp - x_plain| /
+ * max |x_plain| over the 16 species); every other cell keeps the plain
+ * result.  The trusted mode skips the plain reaction phase for such cells and
+ * takes the prediction unchecked. */
+#define MARL_SURR_FEATURES 93
+#define MARL_SURR_RAW_STRIDE 112 /* floats per raw row: 93 features, 16 deltas, pad */
+
+typedef struct marl_surrogate marl_surrogate;
+
+typedef struct marl_surrogate_config {
+    uint32_t max_pairs;   /* capacity of the pair store (rows) */
+    uint32_t batch;       /* training rows per step (multiple of 128) */
+    float lr;             /* Adam step size */
+    float beta1, beta2, adam_eps;
+    uint64_t seed;        /* weight init and batch sampling */
+} marl_surrogate_config;
+
+typedef struct marl_surrogate_eval {
+    uint32_t rows;
+    uint32_t accepted;    /* rows with normwise relative error <= tol */
+    float max_err;
+    float mean_err;
+    float mse_normalised; /* loss on standardised targets */
+} marl_surrogate_eval;
+
+typedef struct marl_surrogate_counters {
+    uint64_t cells;       /* cells updated in surrogate mode */
+    uint64_t speculated;  /* post-transport state equal to the pre-pass state */
+    uint64_t accepted;    /* took the network's prediction */
+    uint64_t rejected;    /* speculated but over tolerance: plain result kept */
+    float max_err;        /* largest normwise error among accepted cells (gated mode) */
+} marl_surrogate_counters;
+
+enum { MARL_SURR_OFF = 0, MARL_SURR_CAPTURE = 1, MARL_SURR_GATED = 2, MARL_SURR_TRUSTED = 3 };
+
+marl_status marl_surrogate_config_default(marl_surrogate_config* out);
+marl_status marl_surrogate_create(const marl_surrogate_config* cfg, marl_surrogate** out);
+void marl_surrogate_destroy(marl_surrogate* s);
+marl_status marl_surrogate_set_stream(marl_surrogate* s, void* cuda_stream);
+/* Rows captured so far. */
+marl_status marl_surrogate_pair_count(marl_surrogate* s, uint32_t* rows);
+/* Raw rows [row0, row0 + n) to the host, MARL_SURR_RAW_STRIDE floats each. */
+marl_status marl_surrogate_download_pairs(marl_surrogate* s, uint32_t row0, uint32_t n, float* out);
+/* Appends raw rows from the host (same layout). */
+marl_status marl_surrogate_upload_pairs(marl_surrogate* s, const float* rows, uint32_t n);
+/* Standardisation statistics over rows [0, n_train) and the standardised
+ * BF16 training matrix of all rows.  Call before training or inference. */
+marl_status marl_surrogate_prepare(marl_surrogate* s, uint32_t n_train);
+/* Adam step size for later training steps. */
+marl_status marl_surrogate_set_lr(marl_surrogate* s, float lr);
+/* `steps` Adam steps on random batches of rows [0, n_train); loss_out
+ * (nullable) receives the mean loss of each step. */
+marl_status marl_surrogate_train(marl_surrogate* s, uint32_t steps, float* loss_out);
+/* Prediction error on rows [row0, row0 + n) against the stored plain deltas. */
+marl_status marl_surrogate_evaluate(marl_surrogate* s, uint32_t row0, uint32_t n, float tol,
+                                    marl_surrogate_eval* out, float* row_err_out /* nullable, n */);
+/* Master weights, FP32, flat: W1[256][128] (inputs 93..127 are zero), b1[256],
+ * W2[256][256], b2[256], W3[16][256], b3[16]; then the standardisation:
+ * in_mean[93], in_std[93], out_mean[16], out_std[16]. */
+#define MARL_SURR_PARAMS (256 * 128 + 256 + 256 * 256 + 256 + 16 * 256 + 16)
+#define MARL_SURR_NORM (93 + 93 + 16 + 16)
+marl_status marl_surrogate_get_weights(marl_surrogate* s, float* params, float* norm);
+marl_status marl_surrogate_set_weights(marl_surrogate* s, const float* params, const float* norm);
+/* One forward + backward pass without an update, for gradient checks: x is
+ * standardised input as BF16 bits [batch][128], t standardised targets
+ * [batch][16]; grads_out gets MARL_SURR_PARAMS floats (same layout as the
+ * weights) of d(loss)/d(param), loss = mean over batch and outputs of
+ * (y - t)^2; y_out (nullable) gets the network output [batch][16]. */
+marl_status marl_surrogate_gradients(marl_surrogate* s, const uint16_t* x, const float* t, uint32_t batch,
+                                     float* grads_out, float* loss_out, float* y_out);
+/* Inference on device memory: x_dev standardised BF16 [n][128]; y_dev gets
+ * the de-standardised deltas as [16][ldy] (species-major).  Asynchronous on
+ * the surrogate's stream. */
+marl_status marl_surrogate_infer_device(marl_surrogate* s, const uint16_t* x_dev, uint32_t n, float* y_dev,
+                                        uint32_t ldy);
+/* Surrogate mode of a context's cell loop (MARL_SURR_*); tol is used by the
+ * gated mode.  The surrogate must outlive its use by the context. */
+marl_status marl_ctx_set_surrogate(marl_ctx* ctx, marl_surrogate* s, int32_t mode, float tol);
+marl_status marl_ctx_surrogate_counters(marl_ctx* ctx, marl_surrogate_counters* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 # Per-file extra flags (default: exact IEEE float semantics).
 EXACT = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
-FLAGS = {}
+FLAGS = {"mlp.cu": ["-prec-div=true", "-prec-sqrt=true", "-ftz=false"]}  # MLP: FMA contraction allowed
 
 
 def nvcc() -> str:

@@ -22,8 +22,11 @@
 // reference's operation order (crates/marl-cell/src/cell.rs:193-369).
 #include <cuda_runtime.h>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "internal.h"
+#include "mlp.h"
 
 namespace marl {
 
@@ -140,6 +143,7 @@ struct CellRunView {
     float* field;
     const float* light;
     uint32_t epoch;
+    const SurrView* sv;  // surrogate modes only
 };
 
 __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j, CellPre& pre) {
@@ -167,11 +171,14 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S,
     pre.light = v.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
 }
 
-// Gather -> tick -> scatter of cell j, after all its dependencies are done.
-__device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
-                            const CellPre& pre) {
+// Gather and transport of cell j (spatial.rs:56-77, cell.rs:223-243): the
+// neighbour mean into S.ext, S.del zeroed then holding the transport deltas,
+// S.x the internal state after transport with the light in slot 15.  Shared
+// by the cell loop and the surrogate's pre-pass, so both produce the same bits
+// from the same field.
+__device__ __forceinline__ void gather_transport(const CellRunView& v, const CellConsts& c, CellScratch& S,
+                                                 const CellPre& pre) {
     const int tid = threadIdx.x;
-    const CellTable& t = *v.t;
     const Grid g = v.g;
     const uint32_t nb = pre.nb;
     const uint32_t P = pre.pos;
@@ -180,7 +187,6 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
                               -(long long)g.X * g.Y};
     const int n = __popc(nb);
-    const uint32_t st0 = pre.state;
     const float light = pre.light;
 
     // Gather: mean of the empty face neighbours (spatial.rs:56-77), summed in
@@ -242,8 +248,13 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
         S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
     }
     S.x[MARL_M_INT - 1][tid] = light;  // cell.rs:243
+}
 
-    // Phase 3: reactions, strictly in slot order (cell.rs:246-285)
+// Phase 3 of CellState::tick: the reactions, strictly in slot order
+// (cell.rs:246-285), on S.x.  Returns the number of active reactions.
+__device__ __forceinline__ int reactions(const CellConsts& c, CellScratch& S) {
+    const int tid = threadIdx.x;
+    const float dt = c.dt;
     const float feps = 1.1920928955078125e-07f;
     int active = 0;
 #pragma unroll 4
@@ -269,6 +280,118 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
         const float flux = fminf(rate * dt, S.x[si][tid]);
         S.x[si][tid] = S.x[si][tid] - flux;
         S.x[pi][tid] = fminf(S.x[pi][tid] + flux, c.c_max);
+    }
+    return active;
+}
+
+// Active-reaction count alone (the maintenance term of cell.rs:291-311),
+// for cells whose reaction phase the surrogate replaces.
+__device__ __forceinline__ int active_reactions(const CellConsts& c, const CellScratch& S) {
+    int active = 0;
+#pragma unroll
+    for (int r = 0; r < MARL_R_MAX; ++r) {
+        const uint4 q = S.rx[r][threadIdx.x];
+        const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF;
+        if (fabsf(__uint_as_float(q.z)) > c.thr && si != pi) ++active;
+    }
+    return active;
+}
+
+// One raw surrogate row from the staged cell after gather_transport:
+// x_T[16], ext[12], light, then per reaction k_m, v_max, k_cat, cofactor flag.
+template <class Put>
+__device__ __forceinline__ void surrogate_features(const CellScratch& S, float light, Put put) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < MARL_M_INT; ++k) put(k, S.x[k][tid]);
+#pragma unroll
+    for (int e = 0; e < MARL_S_EXT; ++e) put(16 + e, S.ext[e][tid]);
+    put(28, light);
+#pragma unroll
+    for (int r = 0; r < MARL_R_MAX; ++r) {
+        const uint4 q = S.rx[r][tid];
+        put(29 + 4 * r, __uint_as_float(q.y));
+        put(30 + 4 * r, __uint_as_float(q.z));
+        put(31 + 4 * r, __uint_as_float(q.w));
+        put(32 + 4 * r, (q.x >> 24) != MARL_NO_COFACTOR ? 1.0f : 0.0f);
+    }
+}
+
+// Gather -> tick -> scatter of cell j, after all its dependencies are done.
+// MODE: kModePlain, kModeCapture (also writes the cell's surrogate training
+// row), kModeGated / kModeTrusted (reaction phase from the surrogate where
+// the pre-pass speculation holds; see SurrView).
+template <int MODE>
+__device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
+                            const CellPre& pre) {
+    const int tid = threadIdx.x;
+    const CellTable& t = *v.t;
+    const Grid g = v.g;
+    const uint32_t nb = pre.nb;
+    const uint32_t P = pre.pos;
+    const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
+    const size_t vox = ((size_t)z * g.Y + y) * g.X + x;
+    const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
+                              -(long long)g.X * g.Y};
+    const int n = __popc(nb);
+    const uint32_t st0 = pre.state;
+    const float dt = c.dt;
+
+    gather_transport(v, c, S, pre);
+
+    int active;
+    if constexpr (MODE == kModePlain) {
+        active = reactions(c, S);
+    } else if constexpr (MODE == kModeCapture) {
+        const SurrView& sv = *v.sv;
+        const bool cap_row = j < sv.raw_rows;
+        float* row = sv.raw + (size_t)j * MARL_SURR_RAW_STRIDE;
+        if (cap_row) surrogate_features(S, pre.light, [&](int f, float val) { row[f] = val; });
+        active = reactions(c, S);
+        if (cap_row) {
+#pragma unroll
+            for (int k = 0; k < MARL_M_INT; ++k) row[MARL_SURR_FEATURES + k] = S.x[k][tid] - row[k];
+        }
+    } else {
+        const SurrView& sv = *v.sv;
+        const size_t cap = t.cap;
+        bool spec = true;
+#pragma unroll
+        for (int k = 0; k < MARL_M_INT; ++k)
+            spec = spec && __float_as_uint(S.x[k][tid]) == __float_as_uint(sv.xt[k * cap + j]);
+        uint8_t status = kSurrNotSpeculated;
+        float err = 0.0f;
+        if (MODE == kModeTrusted && spec) {
+            active = active_reactions(c, S);
+#pragma unroll
+            for (int k = 0; k < MARL_M_INT; ++k)
+                S.x[k][tid] = fminf(fmaxf(S.x[k][tid] + sv.pred[k * cap + j], 0.0f), c.c_max);
+            status = kSurrAccepted;
+        } else {
+            active = reactions(c, S);
+            if (MODE == kModeGated && spec) {
+                // The plain result is the judge: normwise relative error of the
+                // prediction, over the 16 species.
+                float num = 0.0f, den = 0.0f;
+#pragma unroll
+                for (int k = 0; k < MARL_M_INT; ++k) {
+                    const float xs = fminf(fmaxf(sv.xt[k * cap + j] + sv.pred[k * cap + j], 0.0f), c.c_max);
+                    num = fmaxf(num, fabsf(xs - S.x[k][tid]));
+                    den = fmaxf(den, fabsf(S.x[k][tid]));
+                }
+                err = num / fmaxf(den, 1e-6f);
+                if (err <= sv.tol) {
+#pragma unroll
+                    for (int k = 0; k < MARL_M_INT; ++k)
+                        S.x[k][tid] = fminf(fmaxf(sv.xt[k * cap + j] + sv.pred[k * cap + j], 0.0f), c.c_max);
+                    status = kSurrAccepted;
+                } else {
+                    status = kSurrRejected;
+                }
+            }
+        }
+        sv.status[j] = status;
+        sv.err[j] = err;
     }
 
     // Maintenance (cell.rs:291-311)
@@ -378,7 +501,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
 
 // The ticket loop shared by the single-run and the batched kernel.  `resolve`
 // maps a ticket (global cell index) to the lane's run view and local index.
-template <class Resolve>
+template <int MODE, class Resolve>
 __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts& c, uint32_t total, uint32_t* ticket,
                                                uint32_t* err, Resolve resolve) {
     const unsigned FULL = 0xFFFFFFFFu;
@@ -406,7 +529,7 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
                 for (int f = 0; f < 6; ++f)
                     if (pre.dep[f] >= 0 && ld_acquire_u32(&t.done[pre.dep[f]]) != v.epoch) ready = false;
                 if (ready) {
-                    update_cell(v, c, S, j, pre);
+                    update_cell<MODE>(v, c, S, j, pre);
                     // release: this cell's field writes are visible before its done flag
                     st_release_u32(&t.done[j], v.epoch);
                     pending = false;
@@ -430,13 +553,83 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
     }
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constant__ CellLaunch a) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    cell_tick_loop(S, a.k, a.n, a.ticket, a.err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
-        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch};
+    cell_tick_loop<MODE>(S, a.k, a.n, a.ticket, a.err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv};
         j = gi;
     });
+}
+
+// Surrogate pre-pass: gather_transport of every cell on the tick's starting
+// field, with no dependency waits.  A cell none of whose neighbour voxels is
+// written by an earlier cell gets exactly the state the cell loop will see.
+__global__ void __launch_bounds__(kTickThreads) k_surrogate_prepass(const __grid_constant__ CellLaunch a,
+                                                                   const float* __restrict__ norm,
+                                                                   float* __restrict__ xt,
+                                                                   __nv_bfloat16* __restrict__ X) {
+    extern __shared__ __align__(16) unsigned char tick_smem[];
+    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
+    const CellRunView v{&a.t, a.g, a.field, a.light, a.epoch, nullptr};
+    const size_t cap = a.t.cap;
+    for (uint32_t base = blockIdx.x * kTickThreads; base < a.n; base += gridDim.x * kTickThreads) {
+        const uint32_t j = base + threadIdx.x;
+        if (j < a.n) {
+            CellPre pre;
+            stage_cell(v, S, j, pre);
+            gather_transport(v, a.k, S, pre);
+#pragma unroll
+            for (int k = 0; k < MARL_M_INT; ++k) xt[k * cap + j] = S.x[k][threadIdx.x];
+            float f[mlp::kInPad];
+#pragma unroll
+            for (int i = mlp::kIn; i < mlp::kInPad; ++i) f[i] = 0.0f;
+            surrogate_features(S, pre.light, [&](int i, float val) {
+                f[i] = (mlp::feature_transform(i, val) - norm[i]) / norm[mlp::kIn + i];
+            });
+            uint4* row = reinterpret_cast<uint4*>(X + (size_t)j * mlp::kInPad);
+#pragma unroll
+            for (int q = 0; q < mlp::kInPad / 8; ++q) {
+                __nv_bfloat162 h0 = __floats2bfloat162_rn(f[8 * q], f[8 * q + 1]);
+                __nv_bfloat162 h1 = __floats2bfloat162_rn(f[8 * q + 2], f[8 * q + 3]);
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(f[8 * q + 4], f[8 * q + 5]);
+                __nv_bfloat162 h3 = __floats2bfloat162_rn(f[8 * q + 6], f[8 * q + 7]);
+                row[q] = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
+                                    *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
+            }
+        }
+    }
+}
+
+__global__ void k_surrogate_count(const uint8_t* __restrict__ status, const float* __restrict__ err, uint32_t n,
+                                  unsigned long long* __restrict__ counters, uint32_t* __restrict__ max_bits) {
+    __shared__ unsigned int s_cnt[3];
+    __shared__ uint32_t s_max;
+    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_max = 0;
+    __syncthreads();
+    unsigned int spec = 0, acc = 0, rej = 0;
+    uint32_t mx = 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint8_t st = status[j];
+        spec += st != kSurrNotSpeculated;
+        acc += st == kSurrAccepted;
+        rej += st == kSurrRejected;
+        if (st == kSurrAccepted) mx = max(mx, __float_as_uint(err[j]));
+    }
+    atomicAdd(&s_cnt[0], spec);
+    atomicAdd(&s_cnt[1], acc);
+    atomicAdd(&s_cnt[2], rej);
+    atomicMax(&s_max, mx);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (blockIdx.x == 0) atomicAdd(&counters[0], (unsigned long long)n);
+        atomicAdd(&counters[1], (unsigned long long)s_cnt[0]);
+        atomicAdd(&counters[2], (unsigned long long)s_cnt[1]);
+        atomicAdd(&counters[3], (unsigned long long)s_cnt[2]);
+        atomicMax(max_bits, s_max);
+    }
 }
 
 // Batched form: tickets run over the cells of all runs, run-major (run r's
@@ -447,9 +640,9 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc*
                                                                   int parity) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    cell_tick_loop(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    cell_tick_loop<kModePlain>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         const RunDesc& R = runs[find_run(runs, n_runs, gi)];
-        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch};
+        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, nullptr};
         j = gi - R.cell_base;
     });
 }
@@ -855,15 +1048,16 @@ cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
-    if (a.n == 0) return cudaSuccess;
+template <int MODE>
+static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaStream_t s) {
     static int per_sm = 0, configured_device = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(k_cell_tick, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+        cudaError_t e =
+            cudaFuncSetAttribute(k_cell_tick<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick, kTickThreads, kTickSmem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick<MODE>, kTickThreads, kTickSmem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         configured_device = dev;
@@ -874,7 +1068,45 @@ cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
     // ticket holder is running (the dependency waits rely on it).
     const uint32_t resident = (uint32_t)per_sm * (uint32_t)num_sms;
     const uint32_t blocks = blocks_needed < resident ? blocks_needed : resident;
-    k_cell_tick<<<blocks, kTickThreads, kTickSmem, s>>>(a);
+    k_cell_tick<MODE><<<blocks, kTickThreads, kTickSmem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    switch (a.mode) {
+        case kModePlain: return launch_cell_tick_mode<kModePlain>(a, num_sms, s);
+        case kModeCapture: return launch_cell_tick_mode<kModeCapture>(a, num_sms, s);
+        case kModeGated: return launch_cell_tick_mode<kModeGated>(a, num_sms, s);
+        case kModeTrusted: return launch_cell_tick_mode<kModeTrusted>(a, num_sms, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_surrogate_prepass(const CellLaunch& a, const float* norm, float* xt, void* X, int num_sms,
+                                     cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e =
+            cudaFuncSetAttribute(k_surrogate_prepass, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    const uint32_t blocks_needed = (a.n + kTickThreads - 1) / kTickThreads;
+    const uint32_t cap_blocks = (uint32_t)num_sms * 8u;
+    k_surrogate_prepass<<<blocks_needed < cap_blocks ? blocks_needed : cap_blocks, kTickThreads, kTickSmem, s>>>(
+        a, norm, xt, reinterpret_cast<__nv_bfloat16*>(X));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_surrogate_count(const uint8_t* status, const float* err, uint32_t n,
+                                   unsigned long long* counters, uint32_t* max_bits, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t blocks = (n + 255) / 256 < 296 ? (n + 255) / 256 : 296;
+    k_surrogate_count<<<blocks, 256, 0, s>>>(status, err, n, counters, max_bits);
     return cudaGetLastError();
 }
 

@@ -5,6 +5,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -16,6 +17,7 @@
 #include "../../include/marl_cuda.h"
 #include "common.cuh"
 #include "ctx_impl.h"
+#include "surrogate.h"
 #include "internal.h"
 
 using namespace marl;
@@ -145,7 +147,8 @@ void ctx_free(marl_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* dev[] = {c->field[0], c->field[1], c->mask, c->cmap, c->light, c->c4, c->d_hdr, c->d_changes, c->d_block_counts,
                    c->d_edit, c->d_mass_partial, c->d_mass_out, c->d_records, c->d_occ_stage, c->d_seam_mask,
-                   c->d_events_stage};
+                   c->d_events_stage, c->surr_xt, c->surr_pred, c->surr_x, c->surr_status, c->surr_err,
+                   c->surr_counters};
     for (void* p : dev)
         if (p) cudaFree(p);
     void* host[] = {c->h_hdr, c->h_edit, c->h_records, c->h_mass};
@@ -245,8 +248,34 @@ marl_status enqueue_cell_phase(marl_ctx* c) {
     }
     a.epoch = c->epoch;
     CK(cudaMemsetAsync(&c->d_hdr->pad[0], 0, 4, c->stream));
+    uint32_t captured = 0;
+    if (c->surr && c->surr_mode == MARL_SURR_CAPTURE) {
+        marl_surrogate* s = c->surr;
+        captured = s->rows < s->cfg.max_pairs ? std::min(c->n, s->cfg.max_pairs - s->rows) : 0;
+        a.mode = captured ? kModeCapture : kModePlain;
+        a.sv.raw = s->raw + (size_t)s->rows * MARL_SURR_RAW_STRIDE;
+        a.sv.raw_rows = captured;
+    } else if (c->surr && (c->surr_mode == MARL_SURR_GATED || c->surr_mode == MARL_SURR_TRUSTED)) {
+        a.mode = c->surr_mode == MARL_SURR_GATED ? kModeGated : kModeTrusted;
+        CK(launch_surrogate_prepass(a, c->surr->norm, c->surr_xt, c->surr_x, c->num_sms, c->stream));
+        marl_status st = surrogate_infer(c->surr, reinterpret_cast<const __nv_bfloat16*>(c->surr_x), c->n,
+                                         c->surr_pred, c->t.cap, c->stream);
+        if (st) return st;
+        c->launches += 4;
+        a.sv.xt = c->surr_xt;
+        a.sv.pred = c->surr_pred;
+        a.sv.tol = c->surr_tol;
+        a.sv.status = c->surr_status;
+        a.sv.err = c->surr_err;
+    }
     CK(launch_cell_tick(a, c->num_sms, c->stream));
     ++c->launches;
+    if (a.mode == kModeGated || a.mode == kModeTrusted) {
+        CK(launch_surrogate_count(c->surr_status, c->surr_err, c->n, c->surr_counters,
+                                  reinterpret_cast<uint32_t*>(c->surr_counters + 4), c->stream));
+        ++c->launches;
+    }
+    if (captured) c->surr->rows += captured;
     return MARL_OK;
 }
 

@@ -60,6 +60,17 @@ struct marl_ctx {
     uint8_t* d_seam_mask = nullptr;
     marl::DiffusionPlan seam_plan{};
 
+    // Reaction surrogate (marl_ctx_set_surrogate)
+    marl_surrogate* surr = nullptr;
+    int surr_mode = 0;  // MARL_SURR_*
+    float surr_tol = 0.0f;
+    float* surr_xt = nullptr;      // [16][cap] pre-pass post-transport state
+    float* surr_pred = nullptr;    // [16][cap] predicted deltas
+    void* surr_x = nullptr;        // [cap][128] BF16 standardised features
+    uint8_t* surr_status = nullptr;
+    float* surr_err = nullptr;
+    unsigned long long* surr_counters = nullptr;  // cells, speculated, accepted, rejected, max-error bits
+
     uint64_t h2d_bytes = 0;  // transfer counters (engine statistics)
     uint64_t d2h_bytes = 0;
     uint64_t launches = 0;   // kernels enqueued by this context

@@ -104,7 +104,28 @@ cudaError_t launch_moves_batch(const RunDesc* runs, const uint4* items, uint32_t
 cudaError_t launch_births_batch(const RunDesc* runs, const marl_cell* recs, const uint2* slots, uint32_t count,
                                 uint32_t* err, cudaStream_t s);
 
+// Surrogate hooks of the cell loop (modes of k_cell_tick).
+constexpr int kModePlain = 0;
+constexpr int kModeCapture = 1;   // plain, and each cell writes its raw training row
+constexpr int kModeGated = 2;     // prediction checked against the plain reaction phase
+constexpr int kModeTrusted = 3;   // prediction taken unchecked where speculation holds
+constexpr uint8_t kSurrNotSpeculated = 0;
+constexpr uint8_t kSurrAccepted = 1;
+constexpr uint8_t kSurrRejected = 2;
+
+struct SurrView {
+    float* raw = nullptr;        // capture: row j (MARL_SURR_RAW_STRIDE floats) for cell j
+    uint32_t raw_rows = 0;       // capture: cells j < raw_rows write a row
+    const float* xt = nullptr;   // [16][cap] post-transport state from the pre-pass
+    const float* pred = nullptr; // [16][cap] predicted reaction deltas
+    float tol = 0.0f;
+    uint8_t* status = nullptr;   // [cap] kSurr*
+    float* err = nullptr;        // [cap] normwise error of the prediction (gated mode)
+};
+
 struct CellLaunch {
+    int mode = kModePlain;
+    SurrView sv;
     CellTable t;
     uint32_t n;
     Grid g;
@@ -120,6 +141,15 @@ struct CellLaunch {
 
 cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s);
 cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s);
+// Surrogate pre-pass: every cell's gather and transport on the current field
+// (as the cell loop would compute them if no earlier cell had written its
+// neighbourhood): xt [16][cap] and the standardised BF16 features X [cap][128].
+cudaError_t launch_surrogate_prepass(const CellLaunch& a, const float* norm, float* xt, void* X, int num_sms,
+                                     cudaStream_t s);
+// Adds the tick's per-cell statuses to counters[0..3] = cells, speculated,
+// accepted, rejected and the largest accepted error's bits to *max_bits.
+cudaError_t launch_surrogate_count(const uint8_t* status, const float* err, uint32_t n,
+                                   unsigned long long* counters, uint32_t* max_bits, cudaStream_t s);
 // Ordered compaction of Division/Death events into `changes` (after a
 // 64-byte ChangeHeader); block_counts needs compaction_blocks(n) words.
 uint32_t compaction_blocks(uint32_t n);

@@ -1,0 +1,557 @@
+// Tensor-core kernels of the reaction surrogate: a tcgen05 GEMM with the MLP's
+// epilogues, the loss, batch gathering, Adam, and the feature statistics.
+//
+// GEMM form: C[M][N] = A[M][K] * B[N][K]^T with A and B BF16, both K-major
+// (row-major with K contiguous), FP32 accumulation in tensor memory.  One CTA
+// owns a 128-row tile of C and BN columns; K advances in 64-element chunks
+// (one 128-byte swizzle atom of BF16).  All 128 threads copy a chunk of A and
+// B from global memory straight into the 128B-swizzled K-major layout
+// (cp.async, 16 bytes a copy) while the tensor core works on the previous
+// chunk; one elected thread issues the four K=16 tcgen05.mma of a chunk and a
+// tcgen05.commit onto the stage's mbarrier.  The epilogue reads the
+// accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e. rows
+// of the tile) and applies one of:
+//   BIAS_GELU  h = gelu(acc + b): BF16 out, optional BF16 transpose, FP32 z
+//   BIAS_OUT   y = (acc + b) * scale + shift: FP32 out, row- or column-major
+//   GELU_BWD   dz = acc * gelu'(z): BF16 out and transpose, column sums
+//   ATOMIC     out[m][n] += acc (split-K weight gradients), or out[n][m]
+// All three training GEMM shapes (forward, input gradient, weight gradient)
+// are this one form, given transposed copies that the epilogues write.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "mlp.h"
+
+namespace marl {
+namespace mlp {
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;
+constexpr int kGemmThreads = 128;
+
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), leading offset unused for this layout (1), version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu_t(float z, float& t) {
+    const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+    t = tanhf(u);
+    return 0.5f * z * (1.0f + t);
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+    const float t = tanhf(u);
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z * z);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Bounded mbarrier wait for the tensor-core commit of a stage.
+__device__ __forceinline__ bool wait_commit(uint64_t* bar, uint32_t parity, uint32_t* err) {
+    if (mbar_wait_bounded(bar, parity)) return true;
+    if (err) atomicOr(err, kErrTimeoutMbar);
+    return false;
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(const __grid_constant__ GemmArgs a) {
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
+    constexpr uint32_t kTmemCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    constexpr uint32_t kStageA = kBM * 128;
+    constexpr uint32_t kStageB = BN * 128;
+    constexpr uint32_t kStage = kStageA + kStageB;
+    extern __shared__ uint8_t gsm_raw[];
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (smem_u32(gsm_raw) + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
+    const int m0 = blockIdx.x * kBM;
+    const int n0 = blockIdx.y * BN;
+    const int k_begin = blockIdx.z * a.k_per_split;
+    const int k_end = min(a.K, k_begin + a.k_per_split);
+    const int nch = (k_end - k_begin) / kBK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    constexpr uint32_t idesc = idesc_bf16(kBM, BN);
+
+    bool ok = true;
+    for (int c = 0; c < nch; ++c) {
+        const int s = c & 1;
+        if (c >= 2) ok = wait_commit(&bars[s], ((c - 2) >> 1) & 1, a.err) && ok;
+        const uint32_t sa = base + s * kStage, sb = sa + kStageA;
+        const int k0 = k_begin + c * kBK;
+        // A: 128 rows x 8 pieces of 16 bytes; rows beyond M are zero-filled.
+#pragma unroll
+        for (int i = 0; i < (kBM * 8) / kGemmThreads; ++i) {
+            const int p = tid + i * kGemmThreads, r = p >> 3, q = p & 7;
+            const int m = m0 + r;
+            const bool in = m < a.M;
+            const __nv_bfloat16* src = a.A + (size_t)(in ? m : 0) * a.lda + k0 + q * 8;
+            cp_async16_zfill(sa + r * 128 + ((q ^ (r & 7)) << 4), src, in ? 16u : 0u);
+        }
+#pragma unroll
+        for (int i = 0; i < (BN * 8 + kGemmThreads - 1) / kGemmThreads; ++i) {
+            const int p = tid + i * kGemmThreads;
+            if (p < BN * 8) {
+                const int r = p >> 3, q = p & 7;
+                const __nv_bfloat16* src = a.B + (size_t)(n0 + r) * a.ldb + k0 + q * 8;
+                cp_async16_zfill(sb + r * 128 + ((q ^ (r & 7)) << 4), src, 16u);
+            }
+        }
+        cp_async_commit_wait_all();
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk)
+                umma_bf16(tmem, sw128_desc(sa + kk * 32), sw128_desc(sb + kk * 32), idesc, (c > 0 || kk > 0) ? 1u : 0u);
+            umma_commit(&bars[s]);
+        }
+    }
+    if (nch > 0) ok = wait_commit(&bars[(nch - 1) & 1], ((nch - 1) >> 1) & 1, a.err) && ok;
+    tc_fence_after();
+
+    const int row = m0 + warp * 32 + lane;
+    const bool row_ok = row < a.M && ok && nch > 0;
+    const uint32_t t_lane = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int cb = 0; cb < BN; cb += 16) {
+        float v[16];
+        tmem_ld16(t_lane + cb, v);
+        const int n = n0 + cb;
+        if constexpr (EPI == EPI_BIAS_GELU) {
+            float h[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const float z = v[i] + a.bias[n + i];
+                float t;
+                h[i] = gelu_t(z, t);
+                v[i] = z;
+            }
+            if (row_ok) {
+                uint4* o = reinterpret_cast<uint4*>(a.out_bf + (size_t)row * a.ldo + n);
+                o[0] = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
+                                  pack_bf16(h[6], h[7]));
+                o[1] = make_uint4(pack_bf16(h[8], h[9]), pack_bf16(h[10], h[11]), pack_bf16(h[12], h[13]),
+                                  pack_bf16(h[14], h[15]));
+                if (a.out_f) {
+                    float4* zf = reinterpret_cast<float4*>(a.out_f + (size_t)row * a.ldf + n);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) zf[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                }
+                if (a.out_t) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) a.out_t[(size_t)(n + i) * a.ldt + row] = __float2bfloat16_rn(h[i]);
+                }
+            }
+        } else if constexpr (EPI == EPI_BIAS_OUT) {
+            if (row_ok) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    float y = v[i] + a.bias[n + i];
+                    if (a.scale) y = y * a.scale[n + i] + a.shift[n + i];
+                    if (a.out_col_major)
+                        a.out_f[(size_t)(n + i) * a.ldf + row] = y;
+                    else
+                        a.out_f[(size_t)row * a.ldf + n + i] = y;
+                }
+            }
+        } else if constexpr (EPI == EPI_GELU_BWD) {
+            float d[16];
+            if (row_ok) {
+                const float4* zp = reinterpret_cast<const float4*>(a.z_in + (size_t)row * a.ldz + n);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float4 z = zp[i];
+                    d[4 * i] = v[4 * i] * gelu_grad(z.x);
+                    d[4 * i + 1] = v[4 * i + 1] * gelu_grad(z.y);
+                    d[4 * i + 2] = v[4 * i + 2] * gelu_grad(z.z);
+                    d[4 * i + 3] = v[4 * i + 3] * gelu_grad(z.w);
+                }
+                uint4* o = reinterpret_cast<uint4*>(a.out_bf + (size_t)row * a.ldo + n);
+                o[0] = make_uint4(pack_bf16(d[0], d[1]), pack_bf16(d[2], d[3]), pack_bf16(d[4], d[5]),
+                                  pack_bf16(d[6], d[7]));
+                o[1] = make_uint4(pack_bf16(d[8], d[9]), pack_bf16(d[10], d[11]), pack_bf16(d[12], d[13]),
+                                  pack_bf16(d[14], d[15]));
+#pragma unroll
+                for (int i = 0; i < 16; ++i) a.out_t[(size_t)(n + i) * a.ldt + row] = __float2bfloat16_rn(d[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) d[i] = 0.0f;
+            }
+            // bias gradient: column sums of dz over the tile's rows
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float sum = d[i];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+                if (lane == 0 && a.colsum) atomicAdd(&a.colsum[n + i], sum);
+            }
+        } else {  // EPI_ATOMIC
+            if (row_ok) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    if (a.out_col_major)
+                        atomicAdd(&a.out_f[(size_t)(n + i) * a.ldf + row], v[i]);
+                    else
+                        atomicAdd(&a.out_f[(size_t)row * a.ldf + n + i], v[i]);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+template <int BN, int EPI>
+static cudaError_t launch_one(const GemmArgs& a, int splits, cudaStream_t s) {
+    constexpr int smem = 2 * (kBM * 128 + BN * 128) + 1024;
+    static int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
+        cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        configured = dev;
+    }
+    dim3 grid((a.M + kBM - 1) / kBM, a.N / BN, splits);
+    k_gemm<BN, EPI><<<grid, kGemmThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm(const GemmArgs& a, int bn, int epi, cudaStream_t s) {
+    if (a.M <= 0 || a.K <= 0 || a.K % kBK || a.N % bn || a.lda % 8 || a.ldb % 8) return cudaErrorInvalidValue;
+    const int kps = a.k_per_split > 0 ? a.k_per_split : a.K;
+    if (kps % kBK) return cudaErrorInvalidValue;
+    const int splits = (a.K + kps - 1) / kps;
+    if (splits > 1 && epi != EPI_ATOMIC) return cudaErrorInvalidValue;
+    GemmArgs b = a;
+    b.k_per_split = kps;
+#define MARL_GEMM_CASE(BNV, EPIV) \
+    if (bn == BNV && epi == EPIV) return launch_one<BNV, EPIV>(b, splits, s);
+    MARL_GEMM_CASE(256, EPI_BIAS_GELU)
+    MARL_GEMM_CASE(16, EPI_BIAS_OUT)
+    MARL_GEMM_CASE(256, EPI_GELU_BWD)
+    MARL_GEMM_CASE(256, EPI_ATOMIC)
+    MARL_GEMM_CASE(128, EPI_ATOMIC)
+    MARL_GEMM_CASE(16, EPI_ATOMIC)
+#undef MARL_GEMM_CASE
+    return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------- loss -----
+// dY = 2 (y - t) / (B * 16) as BF16 [B][64] (columns 16..63 zero) and its
+// transpose [16][B]; bias gradient of the output layer and the loss sum.
+__global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t, uint32_t B,
+                       __nv_bfloat16* __restrict__ dy, __nv_bfloat16* __restrict__ dyt, float* __restrict__ db3,
+                       float* __restrict__ loss_sum) {
+    __shared__ float s_db[16];
+    __shared__ float s_loss;
+    if (threadIdx.x < 16) s_db[threadIdx.x] = 0.0f;
+    if (threadIdx.x == 0) s_loss = 0.0f;
+    __syncthreads();
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    const float sc = 2.0f / ((float)B * 16.0f);
+    if (r < B) {
+        uint32_t w[8];
+        for (int i = 0; i < 16; i += 2) {
+            const float e0 = y[(size_t)r * 16 + i] - t[(size_t)r * 16 + i];
+            const float e1 = y[(size_t)r * 16 + i + 1] - t[(size_t)r * 16 + i + 1];
+            l += e0 * e0 + e1 * e1;
+            const float g0 = e0 * sc, g1 = e1 * sc;
+            w[i >> 1] = pack_bf16(g0, g1);
+            dyt[(size_t)i * B + r] = __float2bfloat16_rn(g0);
+            dyt[(size_t)(i + 1) * B + r] = __float2bfloat16_rn(g1);
+            atomicAdd(&s_db[i], g0);
+            atomicAdd(&s_db[i + 1], g1);
+        }
+        uint4* o = reinterpret_cast<uint4*>(dy + (size_t)r * 64);
+        o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        for (int i = 2; i < 8; ++i) o[i] = make_uint4(0, 0, 0, 0);
+        atomicAdd(&s_loss, l);
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) atomicAdd(&db3[threadIdx.x], s_db[threadIdx.x]);
+    if (threadIdx.x == 0) atomicAdd(loss_sum, s_loss);
+}
+
+cudaError_t launch_loss(const float* y, const float* t, uint32_t B, __nv_bfloat16* dy, __nv_bfloat16* dyt,
+                        float* db3, float* loss_sum, cudaStream_t s) {
+    k_loss<<<(B + 255) / 256, 256, 0, s>>>(y, t, B, dy, dyt, db3, loss_sum);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ batches ----
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Row r of the batch is training row hash(seed, step, r) mod n_rows: copies
+// its standardised input (BF16 [128]) and target (FP32 [16]), and writes the
+// input transposed ([128][B]) for the first layer's weight gradient.
+__global__ void k_gather_batch(const __nv_bfloat16* __restrict__ X, const float* __restrict__ T, uint32_t n_rows,
+                               uint64_t seed, uint64_t step, uint32_t B, __nv_bfloat16* __restrict__ xb,
+                               __nv_bfloat16* __restrict__ xbt, float* __restrict__ tb) {
+    const uint32_t r = blockIdx.x;
+    if (r >= B) return;
+    const uint32_t src = (uint32_t)(mix64(seed ^ mix64(step * 0x100000001B3ull + r)) % n_rows);
+    const int i = threadIdx.x;  // 0..127
+    const __nv_bfloat16 v = X[(size_t)src * kInPad + i];
+    xb[(size_t)r * kInPad + i] = v;
+    xbt[(size_t)i * B + r] = v;
+    if (i < 16) tb[(size_t)r * 16 + i] = T[(size_t)src * 16 + i];
+}
+
+cudaError_t launch_gather_batch(const __nv_bfloat16* X, const float* T, uint32_t n_rows, uint64_t seed, uint64_t step,
+                                uint32_t B, __nv_bfloat16* xb, __nv_bfloat16* xbt, float* tb, cudaStream_t s) {
+    k_gather_batch<<<B, kInPad, 0, s>>>(X, T, n_rows, seed, step, B, xb, xbt, tb);
+    return cudaGetLastError();
+}
+
+// Transposes a host-provided batch (gradient checks): xbt[i][r] = xb[r][i].
+__global__ void k_transpose_batch(const __nv_bfloat16* __restrict__ xb, uint32_t B, __nv_bfloat16* __restrict__ xbt) {
+    const uint32_t r = blockIdx.x;
+    xbt[(size_t)threadIdx.x * B + r] = xb[(size_t)r * kInPad + threadIdx.x];
+}
+
+cudaError_t launch_transpose_batch(const __nv_bfloat16* xb, uint32_t B, __nv_bfloat16* xbt, cudaStream_t s) {
+    k_transpose_batch<<<B, kInPad, 0, s>>>(xb, B, xbt);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- Adam ----
+// FP32 master parameters p (flat, MARL_SURR_PARAMS) updated from gradients g;
+// then the BF16 copies the GEMMs read: W1, W2, W3, W2^T and W3^T (padded to
+// 64 columns).
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, uint32_t n, float lr, float b1, float b2, float eps, float bc1,
+                       float bc2) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    }
+}
+
+__global__ void k_weights_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ w1,
+                               __nv_bfloat16* __restrict__ w2, __nv_bfloat16* __restrict__ w3,
+                               __nv_bfloat16* __restrict__ w2t, __nv_bfloat16* __restrict__ w3t) {
+    const float* W1 = p + kOffW1;
+    const float* W2 = p + kOffW2;
+    const float* W3 = p + kOffW3;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kHid * kHid; i += gridDim.x * blockDim.x) {
+        const uint32_t o = i / kHid, k = i % kHid;
+        w2[i] = __float2bfloat16_rn(W2[i]);
+        w2t[(size_t)k * kHid + o] = __float2bfloat16_rn(W2[i]);
+        if (i < kHid * kInPad) w1[i] = __float2bfloat16_rn(W1[i]);
+        if (i < kOut * kHid) w3[i] = __float2bfloat16_rn(W3[i]);
+        if (i < kHid * kOutPad) {
+            const uint32_t hi = i / kOutPad, oo = i % kOutPad;  // w3t[hi][oo] = W3[oo][hi]
+            w3t[i] = __float2bfloat16_rn(oo < kOut ? W3[(size_t)oo * kHid + hi] : 0.0f);
+        }
+    }
+}
+
+cudaError_t launch_adam(float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
+                        uint64_t t, cudaStream_t s) {
+    const float bc1 = 1.0f - (float)pow((double)b1, (double)t);
+    const float bc2 = 1.0f - (float)pow((double)b2, (double)t);
+    k_adam<<<256, 256, 0, s>>>(p, g, m, v, kParams, lr, b1, b2, eps, bc1, bc2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_weights_bf16(const float* p, __nv_bfloat16* w1, __nv_bfloat16* w2, __nv_bfloat16* w3,
+                                __nv_bfloat16* w2t, __nv_bfloat16* w3t, cudaStream_t s) {
+    k_weights_bf16<<<256, 256, 0, s>>>(p, w1, w2, w3, w2t, w3t);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------- standardisation ----
+// Sums and sums of squares (FP64) of the transformed features and the
+// targets over raw rows [0, n): acc[0..109) sums, acc[109..218) squares.
+__global__ void k_raw_stats(const float* __restrict__ raw, uint32_t n, double* __restrict__ acc) {
+    constexpr int kCols = kIn + kOut;
+    __shared__ double s[2 * kCols];
+    for (int i = threadIdx.x; i < 2 * kCols; i += blockDim.x) s[i] = 0.0;
+    __syncthreads();
+    const int col = threadIdx.x % 128;
+    if (col < kCols) {
+        double sum = 0.0, sq = 0.0;
+        for (uint32_t r = blockIdx.x * (blockDim.x / 128) + threadIdx.x / 128; r < n;
+             r += gridDim.x * (blockDim.x / 128)) {
+            float v = raw[(size_t)r * MARL_SURR_RAW_STRIDE + col];
+            if (col < kIn) v = feature_transform(col, v);
+            sum += v;
+            sq += (double)v * v;
+        }
+        atomicAdd(&s[col], sum);
+        atomicAdd(&s[kCols + col], sq);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * kCols; i += blockDim.x) atomicAdd(&acc[i], s[i]);
+}
+
+cudaError_t launch_raw_stats(const float* raw, uint32_t n, double* acc, cudaStream_t s) {
+    k_raw_stats<<<296, 512, 0, s>>>(raw, n, acc);
+    return cudaGetLastError();
+}
+
+// Standardised BF16 inputs [n][128] and FP32 targets [n][16] from raw rows.
+// norm: in_mean[93], in_std[93], out_mean[16], out_std[16].
+__global__ void k_standardise(const float* __restrict__ raw, uint32_t n, const float* __restrict__ norm,
+                              __nv_bfloat16* __restrict__ X, float* __restrict__ T) {
+    const uint32_t r = blockIdx.x;
+    if (r >= n) return;
+    const int i = threadIdx.x;  // 0..127
+    const float* row = raw + (size_t)r * MARL_SURR_RAW_STRIDE;
+    float v = 0.0f;
+    if (i < kIn) v = (feature_transform(i, row[i]) - norm[i]) / norm[kIn + i];
+    X[(size_t)r * kInPad + i] = __float2bfloat16_rn(v);
+    if (i < kOut) T[(size_t)r * kOut + i] = (row[kIn + i] - norm[2 * kIn + i]) / norm[2 * kIn + kOut + i];
+}
+
+cudaError_t launch_standardise(const float* raw, uint32_t n, const float* norm, __nv_bfloat16* X, float* T,
+                               cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_standardise<<<n, kInPad, 0, s>>>(raw, n, norm, X, T);
+    return cudaGetLastError();
+}
+
+// Normwise relative error of x_T + prediction against x_T + plain deltas, per
+// row, accumulated: err_out[r], and acc = {accepted count, sum err, max err
+// bits, squared error of standardised outputs}.
+__global__ void k_eval_rows(const float* __restrict__ raw, const float* __restrict__ pred, uint32_t ldp, uint32_t n,
+                            const float* __restrict__ norm, float tol, float c_max, float* __restrict__ err_out,
+                            double* __restrict__ acc, uint32_t* __restrict__ max_bits) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const float* row = raw + (size_t)r * MARL_SURR_RAW_STRIDE;
+    float num = 0.0f, den = 0.0f, se = 0.0f;
+    for (int k = 0; k < kOut; ++k) {
+        const float xt = row[k];
+        const float plain = xt + row[kIn + k];
+        const float d = pred[(size_t)k * ldp + r];
+        const float mlp = fminf(fmaxf(xt + d, 0.0f), c_max);
+        num = fmaxf(num, fabsf(mlp - plain));
+        den = fmaxf(den, fabsf(plain));
+        const float e = (d - row[kIn + k]) / norm[2 * kIn + kOut + k];
+        se += e * e;
+    }
+    const float err = num / fmaxf(den, 1e-6f);
+    if (err_out) err_out[r] = err;
+    atomicAdd(&acc[0], err <= tol ? 1.0 : 0.0);
+    atomicAdd(&acc[1], (double)err);
+    atomicAdd(&acc[2], (double)se);
+    atomicMax(max_bits, __float_as_uint(err));
+}
+
+cudaError_t launch_eval_rows(const float* raw, const float* pred, uint32_t ldp, uint32_t n, const float* norm,
+                             float tol, float c_max, float* err_out, double* acc, uint32_t* max_bits,
+                             cudaStream_t s) {
+    k_eval_rows<<<(n + 255) / 256, 256, 0, s>>>(raw, pred, ldp, n, norm, tol, c_max, err_out, acc, max_bits);
+    return cudaGetLastError();
+}
+
+// Initial weights: uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) from a counter
+// hash; W1 columns 93..127 and all biases zero.
+__global__ void k_init_weights(float* __restrict__ p, uint64_t seed) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        const double u = (double)(mix64(seed ^ mix64(i)) >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+        float v = 0.0f;
+        if (i < kOffB1) {
+            v = (i % kInPad) < kIn ? (float)(u / sqrt((double)kIn)) : 0.0f;
+        } else if (i >= kOffW2 && i < kOffB2) {
+            v = (float)(u / sqrt((double)kHid));
+        } else if (i >= kOffW3 && i < kOffB3) {
+            v = (float)(u / sqrt((double)kHid));
+        }
+        p[i] = v;
+    }
+}
+
+cudaError_t launch_init_weights(float* p, uint64_t seed, cudaStream_t s) {
+    k_init_weights<<<256, 256, 0, s>>>(p, seed);
+    return cudaGetLastError();
+}
+
+}  // namespace mlp
+}  // namespace marl

@@ -132,6 +132,27 @@ class MarlError(RuntimeError):
         super().__init__(f"{where}: {self.status_name} ({status}) {message}".strip())
 
 
+class SurrogateConfig(ctypes.Structure):
+    _fields_ = [("max_pairs", c_uint32), ("batch", c_uint32), ("lr", c_float), ("beta1", c_float),
+                ("beta2", c_float), ("adam_eps", c_float), ("seed", c_uint64)]
+
+
+class SurrogateEval(ctypes.Structure):
+    _fields_ = [("rows", c_uint32), ("accepted", c_uint32), ("max_err", c_float), ("mean_err", c_float),
+                ("mse_normalised", c_float)]
+
+
+class SurrogateCounters(ctypes.Structure):
+    _fields_ = [("cells", c_uint64), ("speculated", c_uint64), ("accepted", c_uint64), ("rejected", c_uint64),
+                ("max_err", c_float)]
+
+
+SURR_FEATURES = 93
+SURR_RAW_STRIDE = 112
+SURR_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 16 * 256 + 16
+SURR_NORM = 93 + 93 + 16 + 16
+SURR_OFF, SURR_CAPTURE, SURR_GATED, SURR_TRUSTED = 0, 1, 2, 3
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmarl_cuda.so")
 
@@ -153,6 +174,11 @@ EXPORTED = [
     "marl_batch_set_tile", "marl_batch_get_tile", "marl_batch_autotune", "marl_batch_set_graph", "marl_batch_step",
     "marl_batch_run_count", "marl_batch_stats_get", "marl_batch_get_cells", "marl_batch_get_field",
     "marl_batch_get_light", "marl_batch_counters",
+    "marl_surrogate_config_default", "marl_surrogate_create", "marl_surrogate_destroy", "marl_surrogate_set_stream",
+    "marl_surrogate_pair_count", "marl_surrogate_download_pairs", "marl_surrogate_upload_pairs",
+    "marl_surrogate_prepare", "marl_surrogate_set_lr", "marl_surrogate_train", "marl_surrogate_evaluate",
+    "marl_surrogate_get_weights", "marl_surrogate_set_weights", "marl_surrogate_gradients",
+    "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
 ]
 
 _lib = None
@@ -227,6 +253,23 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_batch_get_field": (c_int32, [P, c_uint32, P]),
         "marl_batch_get_light": (c_int32, [P, c_uint32, P]),
         "marl_batch_counters": (c_int32, [P, POINTER(Counters)]),
+        "marl_surrogate_config_default": (c_int32, [POINTER(SurrogateConfig)]),
+        "marl_surrogate_create": (c_int32, [POINTER(SurrogateConfig), POINTER(c_void_p)]),
+        "marl_surrogate_destroy": (None, [P]),
+        "marl_surrogate_set_stream": (c_int32, [P, P]),
+        "marl_surrogate_pair_count": (c_int32, [P, POINTER(c_uint32)]),
+        "marl_surrogate_download_pairs": (c_int32, [P, c_uint32, c_uint32, P]),
+        "marl_surrogate_upload_pairs": (c_int32, [P, P, c_uint32]),
+        "marl_surrogate_prepare": (c_int32, [P, c_uint32]),
+        "marl_surrogate_set_lr": (c_int32, [P, c_float]),
+        "marl_surrogate_train": (c_int32, [P, c_uint32, P]),
+        "marl_surrogate_evaluate": (c_int32, [P, c_uint32, c_uint32, c_float, POINTER(SurrogateEval), P]),
+        "marl_surrogate_get_weights": (c_int32, [P, P, P]),
+        "marl_surrogate_set_weights": (c_int32, [P, P, P]),
+        "marl_surrogate_gradients": (c_int32, [P, P, P, c_uint32, P, POINTER(c_float), P]),
+        "marl_surrogate_infer_device": (c_int32, [P, P, c_uint32, P, c_uint32]),
+        "marl_ctx_set_surrogate": (c_int32, [P, P, c_int32, c_float]),
+        "marl_ctx_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -637,3 +680,119 @@ class Batch:
         out = np.empty((Z, Y, X), np.float32)
         _check(self.lib.marl_batch_get_light(self.h, run, _ptr(out)), "marl_batch_get_light")
         return out
+
+
+class Surrogate:
+    """Learned reaction surrogate (marl_surrogate): pair store, training on the
+    GPU, evaluation and inference.  See include/marl_cuda.h for the features."""
+
+    def __init__(self, max_pairs: int | None = None, batch: int | None = None, lr: float | None = None,
+                 seed: int | None = None):
+        self.lib = load()
+        cfg = SurrogateConfig()
+        _check(self.lib.marl_surrogate_config_default(ctypes.byref(cfg)), "marl_surrogate_config_default")
+        if max_pairs is not None:
+            cfg.max_pairs = max_pairs
+        if batch is not None:
+            cfg.batch = batch
+        if lr is not None:
+            cfg.lr = lr
+        if seed is not None:
+            cfg.seed = seed
+        self.cfg = cfg
+        h = c_void_p()
+        _check(self.lib.marl_surrogate_create(ctypes.byref(cfg), ctypes.byref(h)), "marl_surrogate_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.marl_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib.marl_surrogate_set_stream(self.h, c_void_p(stream_ptr)), "marl_surrogate_set_stream")
+
+    def pair_count(self) -> int:
+        n = c_uint32()
+        _check(self.lib.marl_surrogate_pair_count(self.h, ctypes.byref(n)), "marl_surrogate_pair_count")
+        return n.value
+
+    def download_pairs(self, row0: int = 0, n: int | None = None) -> np.ndarray:
+        n = self.pair_count() - row0 if n is None else n
+        out = np.zeros((max(n, 1), SURR_RAW_STRIDE), np.float32)
+        _check(self.lib.marl_surrogate_download_pairs(self.h, row0, n, _ptr(out)), "marl_surrogate_download_pairs")
+        return out[:n]
+
+    def upload_pairs(self, rows: np.ndarray) -> None:
+        r = np.ascontiguousarray(rows, np.float32).reshape(-1, SURR_RAW_STRIDE)
+        _check(self.lib.marl_surrogate_upload_pairs(self.h, _ptr(r), r.shape[0]), "marl_surrogate_upload_pairs")
+
+    def prepare(self, n_train: int) -> None:
+        _check(self.lib.marl_surrogate_prepare(self.h, n_train), "marl_surrogate_prepare")
+
+    def set_lr(self, lr: float) -> None:
+        _check(self.lib.marl_surrogate_set_lr(self.h, lr), "marl_surrogate_set_lr")
+
+    def train(self, steps: int) -> np.ndarray:
+        loss = np.zeros(max(steps, 1), np.float32)
+        _check(self.lib.marl_surrogate_train(self.h, steps, _ptr(loss)), "marl_surrogate_train")
+        return loss[:steps]
+
+    def evaluate(self, row0: int, n: int, tol: float = 1e-3, per_row: bool = False):
+        ev = SurrogateEval()
+        errs = np.zeros(n, np.float32) if per_row else None
+        _check(self.lib.marl_surrogate_evaluate(self.h, row0, n, tol, ctypes.byref(ev),
+                                                _ptr(errs) if per_row else None), "marl_surrogate_evaluate")
+        out = {name: getattr(ev, name) for name, _ in SurrogateEval._fields_}
+        if per_row:
+            out["row_err"] = errs
+        return out
+
+    def get_weights(self) -> tuple[np.ndarray, np.ndarray]:
+        p = np.zeros(SURR_PARAMS, np.float32)
+        nrm = np.zeros(SURR_NORM, np.float32)
+        _check(self.lib.marl_surrogate_get_weights(self.h, _ptr(p), _ptr(nrm)), "marl_surrogate_get_weights")
+        return p, nrm
+
+    def set_weights(self, params: np.ndarray | None = None, norm: np.ndarray | None = None) -> None:
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        nrm = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        _check(self.lib.marl_surrogate_set_weights(self.h, _ptr(p) if p is not None else None,
+                                                   _ptr(nrm) if nrm is not None else None),
+               "marl_surrogate_set_weights")
+
+    def gradients(self, x_bf16: np.ndarray, t: np.ndarray):
+        """One forward + backward without an update: (grads, loss, y)."""
+        x = np.ascontiguousarray(x_bf16, np.uint16)
+        tt = np.ascontiguousarray(t, np.float32)
+        B = x.shape[0]
+        g = np.zeros(SURR_PARAMS, np.float32)
+        y = np.zeros((B, 16), np.float32)
+        loss = c_float()
+        _check(self.lib.marl_surrogate_gradients(self.h, _ptr(x), _ptr(tt), B, _ptr(g), ctypes.byref(loss), _ptr(y)),
+               "marl_surrogate_gradients")
+        return g, loss.value, y
+
+    def infer_device(self, x_ptr: int, n: int, y_ptr: int, ldy: int) -> None:
+        _check(self.lib.marl_surrogate_infer_device(self.h, c_void_p(x_ptr), n, c_void_p(y_ptr), ldy),
+               "marl_surrogate_infer_device")
+
+
+def ctx_set_surrogate(ctx_handle, surrogate: "Surrogate | None", mode: int, tol: float = 1e-3) -> None:
+    """marl_ctx_set_surrogate on a context handle (Context.h or marl_engine_ctx)."""
+    lib = load()
+    _check(lib.marl_ctx_set_surrogate(ctx_handle, surrogate.h if surrogate is not None else None, mode, tol),
+           "marl_ctx_set_surrogate")
+
+
+def ctx_surrogate_counters(ctx_handle) -> dict:
+    lib = load()
+    c = SurrogateCounters()
+    _check(lib.marl_ctx_surrogate_counters(ctx_handle, ctypes.byref(c)), "marl_ctx_surrogate_counters")
+    return {name: getattr(c, name) for name, _ in SurrogateCounters._fields_}
