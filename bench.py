@@ -35,6 +35,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "marl-ochre_b200"))
 
@@ -122,6 +124,25 @@ class ClockSampler:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def max_over_ranks(values, dist, device) -> list:
+    """Element-wise maximum of per-rank timings (the slowest replica sets the
+    job's time); identity without a process group."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def replica_rates(steps: int, world: int, dev_s: float, wall_s: float) -> tuple[float, float]:
+    """Whole-job ticks/s of `world` independent replicas of `steps` ticks each,
+    from the maximum device time and the maximum wall time over ranks."""
+    total = steps * world
+    return total / dev_s, total / wall_s
 
 
 def cpu_baseline(budget_s: float = 15.0, max_ticks: int = 60) -> dict:
@@ -219,6 +240,163 @@ def diffusion_roofline(marl, torch, engine, stream, fixed_tile=None) -> dict:
             "l2": "flushed between groups of 10 substeps (one tick's worth)"}
 
 
+ENSEMBLE_GRIDS = [(64, 64, 32), (96, 96, 48), (128, 128, 64), (128, 128, 96)]
+MLP_FLOP_PER_CELL = 2 * (93 * 256 + 256 * 256 + 256 * 16)  # algorithmic forward FLOPs (93 inputs)
+
+
+def ensemble_leg(marl, torch, stream, ticks: int = 30, warmup: int = 3) -> dict:
+    """Batched ensemble: 64 runs (seeds 0-63), 16 each of four grid sizes, one
+    launch per phase for all runs, graph-captured device tick."""
+    runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
+    b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=1 << 16)
+    b.set_stream(stream.cuda_stream)
+    us = b.autotune(3)
+    b.step(warmup)
+    torch.cuda.synchronize()
+    c0 = b.counters()
+    t0 = time.perf_counter()
+    b.step(ticks)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    c1 = b.counters()
+    dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
+    pop = sum(b.stats(r)["population"] for r in range(len(runs)))
+    b.close()
+    return {"workload": "64 runs, seeds 0-63, 16 each of 64x64x32, 96x96x48, 128x128x64, 128x128x96; "
+                        f"ticks {warmup + 1}..{warmup + ticks}",
+            "run_ticks_per_s": len(runs) * ticks / dev_s, "e2e_run_ticks_per_s": len(runs) * ticks / wall,
+            "ms_per_batch_tick": 1000.0 * dev_s / ticks, "population_end": int(pop),
+            "autotune_us_per_batched_substep": us,
+            "note": "device time (CUDA events on the batch stream) of the graph-replayed device ticks and edit "
+                    "copies; e2e adds the host fate step of all runs on worker threads"}
+
+
+def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int = 10_000_000) -> dict:
+    """Learned reaction surrogate: pairs captured from the plain cell kernel on
+    seeded 128x128x64 default runs, trained on the GPU, evaluated on held-out
+    rows and in the tick (gated at 1e-3 and trusted), against the plain tick
+    from the same state."""
+    t_start = time.perf_counter()
+    p = marl.default_params()
+    s = marl.Surrogate(max_pairs=target_pairs, batch=8192, lr=2e-3, seed=5)
+    s.set_stream(stream.cuda_stream)
+    seed, cap_ticks = 100, 0
+    while s.pair_count() < target_pairs and time.perf_counter() - t_start < budget_s / 3:
+        e = marl.Engine(DIMS, p, rng_seed=seed, seed_count=SEED_COUNT, cell_capacity=1 << 20)
+        e.set_stream(stream.cuda_stream)
+        e.step(20)
+        marl.ctx_set_surrogate(e.lib.marl_engine_ctx(e.h), s, marl.SURR_CAPTURE)
+        while s.pair_count() < target_pairs and time.perf_counter() - t_start < budget_s / 3:
+            e.step(20)
+            cap_ticks += 20
+            if e.stats()["tick"] >= 600:
+                break
+        marl.ctx_set_surrogate(e.lib.marl_engine_ctx(e.h), None, marl.SURR_OFF)
+        e.close()
+        seed += 1
+    t_cap = time.perf_counter() - t_start
+    n = s.pair_count()
+    n_train = int(0.95 * n)
+    s.prepare(n_train)
+    t0 = time.perf_counter()
+    steps = 0
+    losses = []
+    train_budget = budget_s / 3
+    while time.perf_counter() - t0 < train_budget:
+        if steps == 4000:
+            s.set_lr(5e-4)
+        losses.append(s.train(500))
+        steps += 500
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    held = s.evaluate(n_train, n - n_train, tol=1e-3)
+    raw = s.download_pairs(n_train, min(n - n_train, 200_000))
+    d = raw[:, 93:109]
+    plain = raw[:, :16] + d
+    zero_ok = float(((np.abs(d).max(1) / np.maximum(np.abs(plain).max(1), 1e-6)) <= 1e-3).mean())
+
+    # Inference kernels alone: three tcgen05 GEMM launches on n_cells rows.
+    n_cells = 300_000
+    x = torch.randn(n_cells, 128, device="cuda").to(torch.bfloat16)
+    x[:, 93:] = 0
+    y = torch.empty(16, n_cells, device="cuda")
+    for _ in range(3):
+        s.infer_device(x.data_ptr(), n_cells, y.data_ptr(), n_cells)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    ev0.record(stream)
+    for _ in range(reps):
+        s.infer_device(x.data_ptr(), n_cells, y.data_ptr(), n_cells)
+    ev1.record(stream)
+    ev1.synchronize()
+    infer_s = ev0.elapsed_time(ev1) / 1000.0 / reps
+    tflops = MLP_FLOP_PER_CELL * n_cells / infer_s / 1e12
+
+    # The tick in each mode, from one state of a long default run.
+    e = marl.Engine(DIMS, p, rng_seed=SEED, seed_count=SEED_COUNT, cell_capacity=1 << 20)
+    e.set_stream(stream.cuda_stream)
+    e.step(400)
+    field, cells, light = e.field(), e.cells(), e.light()
+    e.close()
+    modes = {}
+    finals = {}
+    for name, mode in (("plain", marl.SURR_OFF), ("gated", marl.SURR_GATED), ("trusted", marl.SURR_TRUSTED)):
+        # one cell phase from the identical state, for the error against the plain kernel
+        ctx = marl.Context(DIMS, p, cell_capacity=len(cells))
+        ctx.upload_field(field)
+        ctx.upload_light(light)
+        ctx.upload_cells(cells)
+        if mode != marl.SURR_OFF:
+            marl.ctx_set_surrogate(ctx.h, s, mode, 1e-3)
+        ctx.cell_phase()
+        finals[name] = ctx.download_cells()["internal"]
+        ctx.close()
+        # whole ticks through the engine, device time
+        eng = marl.Engine(DIMS, p, rng_seed=SEED, field=field, cells=cells, cell_capacity=1 << 20)
+        eng.set_stream(stream.cuda_stream)
+        h = eng.lib.marl_engine_ctx(eng.h)
+        if mode != marl.SURR_OFF:
+            marl.ctx_set_surrogate(h, s, mode, 1e-3)
+        eng.step(3)
+        torch.cuda.synchronize()
+        c0 = eng.counters()
+        k = 20
+        eng.step(k)
+        c1 = eng.counters()
+        cnt = marl.ctx_surrogate_counters(h) if mode != marl.SURR_OFF else None
+        modes[name] = {"ticks_per_s": k / ((c1["device_us"] - c0["device_us"]) / 1e6),
+                       "counters": None if cnt is None else {kk: (float(v) if isinstance(v, float) else int(v))
+                                                             for kk, v in cnt.items()}}
+        eng.close()
+    for name in ("gated", "trusted"):
+        a, b = finals[name], finals["plain"]
+        err = np.abs(a - b).max(1) / np.maximum(np.abs(b).max(1), 1e-6)
+        modes[name]["cell_phase_rel_err_max"] = float(err.max())
+        modes[name]["cell_phase_cells_within_1e-3"] = float((err <= 1e-3).mean())
+    s.close()
+    return {
+        "workload": f"pairs from {seed - 100} seeded 128x128x64 default runs (ticks 21..<=600), "
+                    f"{n} rows, last 5% held out; tick comparison from tick 400 of the seed-{SEED} run "
+                    f"({len(cells)} cells)",
+        "pairs": n, "capture_s": t_cap, "train_steps": steps, "train_batch": 8192, "train_s": t_train,
+        "loss_first": float(losses[0][:20].mean()), "loss_last": float(losses[-1][-100:].mean()),
+        "held_out": {"rows": held["rows"], "accepted_frac_1e-3": held["accepted"] / held["rows"],
+                     "mean_err": held["mean_err"], "zero_delta_accepted_frac_1e-3": zero_ok},
+        "mlp_infer": {"cells": n_cells, "us": infer_s * 1e6, "tflops_algorithmic": tflops,
+                      "peak_tflops": peaks_bf16(), "frac": tflops / peaks_bf16(),
+                      "flop_per_cell": MLP_FLOP_PER_CELL},
+        "tick_modes": modes,
+    }
+
+
+def peaks_bf16() -> float:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -229,6 +407,8 @@ def main() -> int:
     ap.add_argument("--tile", type=int, nargs=2, metavar=("TILE", "ZC"),
                     help="fixed diffusion tile index and z-chunk instead of the autotuner (for launch lists)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the separate diffusion timing")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -288,18 +468,19 @@ def main() -> int:
     dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
     launches = c1["kernel_launches"] - c0["kernel_launches"]
     st = eng.stats()
+    dev_s, wall = max_over_ranks([dev_s, wall], dist, "cuda")
     if dist:
-        t = torch.tensor([dev_s, wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_s, wall = float(t[0]), float(t[1])
         dist.barrier()
-    total_ticks = args.steps * world
-    value = total_ticks / dev_s
-    e2e = total_ticks / wall
+    value, e2e = replica_rates(args.steps, world, dev_s, wall)
 
     roof = None
     if rank == 0 and not args.no_roofline:
         roof = diffusion_roofline(marl, torch, eng, stream, tuple(args.tile) if args.tile else None)
+    ens = surr = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        ens = ensemble_leg(marl, torch, stream)
+    if rank == 0 and world == 1 and not args.no_surrogate:
+        surr = surrogate_leg(marl, torch, stream)
     if rank == 0:
         base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline()
         line = {
@@ -319,6 +500,8 @@ def main() -> int:
                     "api": "marl_engine_step (C ABI), wall clock per tick"},
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "ensemble": ens,
+            "surrogate": surr,
         }
         print(json.dumps(line), flush=True)
     eng.close()

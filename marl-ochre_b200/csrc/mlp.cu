@@ -12,6 +12,7 @@
 // accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e. rows
 // of the tile) and applies one of:
 //   BIAS_GELU  h = gelu(acc + b): BF16 out, optional BF16 transpose, FP32 z
+//              (BIAS_GELU_FAST: the same with the hardware tanh, for inference)
 //   BIAS_OUT   y = (acc + b) * scale + shift: FP32 out, row- or column-major
 //   GELU_BWD   dz = acc * gelu'(z): BF16 out and transpose, column sums
 //   ATOMIC     out[m][n] += acc (split-K weight gradients), or out[n][m]
@@ -86,6 +87,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 __device__ __forceinline__ float gelu_t(float z, float& t) {
     const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
     t = tanhf(u);
+    return 0.5f * z * (1.0f + t);
+}
+// Inference form: the hardware tanh approximation (MUFU), max relative error
+// about 2^-11, below the BF16 rounding the activation goes through next.
+__device__ __forceinline__ float gelu_fast(float z) {
+    const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
     return 0.5f * z * (1.0f + t);
 }
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -188,13 +197,17 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(const __grid_constant__ G
         float v[16];
         tmem_ld16(t_lane + cb, v);
         const int n = n0 + cb;
-        if constexpr (EPI == EPI_BIAS_GELU) {
+        if constexpr (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_FAST) {
             float h[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const float z = v[i] + a.bias[n + i];
-                float t;
-                h[i] = gelu_t(z, t);
+                if constexpr (EPI == EPI_BIAS_GELU_FAST) {
+                    h[i] = gelu_fast(z);
+                } else {
+                    float t;
+                    h[i] = gelu_t(z, t);
+                }
                 v[i] = z;
             }
             if (row_ok) {
@@ -301,6 +314,7 @@ cudaError_t launch_gemm(const GemmArgs& a, int bn, int epi, cudaStream_t s) {
 #define MARL_GEMM_CASE(BNV, EPIV) \
     if (bn == BNV && epi == EPIV) return launch_one<BNV, EPIV>(b, splits, s);
     MARL_GEMM_CASE(256, EPI_BIAS_GELU)
+    MARL_GEMM_CASE(256, EPI_BIAS_GELU_FAST)
     MARL_GEMM_CASE(16, EPI_BIAS_OUT)
     MARL_GEMM_CASE(256, EPI_GELU_BWD)
     MARL_GEMM_CASE(256, EPI_ATOMIC)

@@ -35,7 +35,7 @@ __device__ __forceinline__ float feature_transform(int f, float v) {
 }
 #endif
 
-enum Epi : int { EPI_BIAS_GELU = 0, EPI_BIAS_OUT = 1, EPI_GELU_BWD = 2, EPI_ATOMIC = 3 };
+enum Epi : int { EPI_BIAS_GELU = 0, EPI_BIAS_OUT = 1, EPI_GELU_BWD = 2, EPI_ATOMIC = 3, EPI_BIAS_GELU_FAST = 4 };
 
 struct GemmArgs {
     const __nv_bfloat16* A = nullptr;  // [M][lda], K contiguous

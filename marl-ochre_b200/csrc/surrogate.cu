@@ -197,10 +197,10 @@ marl_status surrogate_infer(marl_surrogate* s, const __nv_bfloat16* x, uint32_t 
     a.A = x, a.lda = mlp::kInPad, a.B = s->w1, a.ldb = mlp::kInPad;
     a.M = (int)n, a.N = mlp::kHid, a.K = mlp::kInPad;
     a.bias = s->p + mlp::kOffB1, a.out_bf = s->ih1, a.ldo = mlp::kHid;
-    SST(gemm(a, 256, mlp::EPI_BIAS_GELU, stream));
+    SST(gemm(a, 256, mlp::EPI_BIAS_GELU_FAST, stream));
     a.A = s->ih1, a.lda = mlp::kHid, a.B = s->w2, a.ldb = mlp::kHid, a.K = mlp::kHid;
     a.bias = s->p + mlp::kOffB2, a.out_bf = s->ih2;
-    SST(gemm(a, 256, mlp::EPI_BIAS_GELU, stream));
+    SST(gemm(a, 256, mlp::EPI_BIAS_GELU_FAST, stream));
     mlp::GemmArgs o;
     o.err = s->d_err;
     o.A = s->ih2, o.lda = mlp::kHid, o.B = s->w3, o.ldb = mlp::kHid;

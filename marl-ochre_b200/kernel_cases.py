@@ -3,6 +3,9 @@
     python marl-ochre_b200/kernel_cases.py diffusion [--dims 128 128 64] [--tile 6] [--zc 16] [--substeps 8]
     python marl-ochre_b200/kernel_cases.py cells [--dims 128 128 64] [--cells 90] [--reps 4]
     python marl-ochre_b200/kernel_cases.py light [--dims 128 128 64] [--reps 4]
+    python marl-ochre_b200/kernel_cases.py mlp [--rows 300000] [--reps 4]
+    python marl-ochre_b200/kernel_cases.py engine [--ticks 1000]   (seed-42 default run; one
+        k_cell_tick launch per tick, so `-k regex:k_cell_tick -s <ticks-1> -c 1` captures the last)
 
 Each case builds a context, uploads seeded synthetic state and runs the kernel
 a few times.  Under `ncu -k regex:<kernel> -s <n> -c 1` that captures one
@@ -61,9 +64,37 @@ def random_cells(dims, n: int, rng: np.random.Generator) -> np.ndarray:
     return c
 
 
+def mlp_case(rows: int, reps: int, rng: np.random.Generator) -> int:
+    """Surrogate inference (three tcgen05 GEMM launches) on `rows` random
+    standardised feature rows, with random weights."""
+    import torch
+
+    s = marl.Surrogate(max_pairs=128, batch=128)
+    params = np.zeros(marl.SURR_PARAMS, np.float32)
+    params[: 256 * 128] = rng.normal(0, 0.1, 256 * 128)
+    params[256 * 128 + 256: 256 * 128 + 256 + 65536] = rng.normal(0, 0.06, 65536)
+    params[-16 - 4096: -16] = rng.normal(0, 0.06, 4096)
+    norm = np.zeros(marl.SURR_NORM, np.float32)
+    norm[93:186] = 1.0
+    norm[202:218] = 1.0
+    s.set_weights(params, norm)
+    x = torch.randn(rows, 128, device="cuda").to(torch.bfloat16)
+    x[:, 93:] = 0
+    y = torch.empty(16, rows, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(reps):
+        s.infer_device(x.data_ptr(), rows, y.data_ptr(), rows)
+    torch.cuda.synchronize()
+    print(f"mlp ok: rows={rows} reps={reps} finite={bool(torch.isfinite(y).all())}")
+    s.close()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["diffusion", "cells", "light"])
+    ap.add_argument("case", choices=["diffusion", "cells", "light", "mlp", "engine"])
+    ap.add_argument("--ticks", type=int, default=1000, help="engine: ticks of the seed-42 default run")
+    ap.add_argument("--rows", type=int, default=300_000, help="mlp: rows (cells) per inference")
     ap.add_argument("--dims", type=int, nargs=3, default=[128, 128, 64])
     ap.add_argument("--tile", type=int, default=-1, help="diffusion tile index (-1: autotune)")
     ap.add_argument("--zc", type=int, default=16)
@@ -74,6 +105,13 @@ def main() -> int:
     dims = tuple(a.dims)
     X, Y, Z = dims
     rng = np.random.default_rng(1)
+    if a.case == "mlp":
+        return mlp_case(a.rows, a.reps, rng)
+    if a.case == "engine":
+        e = marl.Engine(dims, marl.default_params(), rng_seed=42, seed_count=30, cell_capacity=1 << 20)
+        e.step(a.ticks)
+        print(f"engine ok: dims={dims} ticks={a.ticks} stats={e.stats()}")
+        return 0
     field = rng.random((Z, Y, X, 12), dtype=np.float32)
     if a.case == "cells":
         cells = random_cells(dims, a.cells, rng)
