@@ -177,7 +177,7 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S,
 // by the cell loop and the surrogate's pre-pass, so both produce the same bits
 // from the same field.
 __device__ __forceinline__ void gather_transport(const CellRunView& v, const CellConsts& c, CellScratch& S,
-                                                 const CellPre& pre) {
+                                                 const CellPre& pre, float4 (&nv)[6][3]) {
     const int tid = threadIdx.x;
     const Grid g = v.g;
     const uint32_t nb = pre.nb;
@@ -200,6 +200,7 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
         if (!((nb >> f) & 1u)) continue;
         const float* src = v.field + (size_t)((long long)vox + off[f]) * 12;
         const float4 q0 = ld4(src), q1 = ld4(src + 4), q2 = ld4(src + 8);
+        nv[f][0] = q0, nv[f][1] = q1, nv[f][2] = q2;
         const float vals[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 #pragma unroll
         for (int s = 0; s < 12; ++s) acc[s] = acc[s] + vals[s];
@@ -337,7 +338,10 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     const uint32_t st0 = pre.state;
     const float dt = c.dt;
 
-    gather_transport(v, c, S, pre);
+    // The gathered neighbour values are also the scatter's starting values:
+    // no other cell touches N(j) while this cell holds it.
+    float4 nv[6][3];
+    gather_transport(v, c, S, pre, nv);
 
     int active;
     if constexpr (MODE == kModePlain) {
@@ -462,15 +466,6 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     // Scatter: split deltas over the same neighbours, clamp after each add
     // (spatial.rs:87-110, field.rs:57-62).
     if (n > 0) {
-        // The neighbours' current values are loaded together before any
-        // store: no other cell touches N(j) while this cell holds it.
-        float4 nv[6][3];
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            if (!((nb >> f) & 1u)) continue;
-            const float* src = v.field + (size_t)((long long)vox + off[f]) * 12;
-            nv[f][0] = ld4(src), nv[f][1] = ld4(src + 4), nv[f][2] = ld4(src + 8);
-        }
         float split[12];
         if (n == 1 || n == 2 || n == 4) {
             const float inv = n == 1 ? 1.0f : (n == 2 ? 0.5f : 0.25f);
@@ -520,15 +515,24 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
             resolve(gi, v, j);
             stage_cell(v, S, j, pre);
         }
+        // Dependencies not yet seen finished (bit f: face f).  A poll loads
+        // them with relaxed loads, all in flight together; once every one has
+        // been seen, one acquire fence orders the update after the writers.
+        uint32_t remaining = 0;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) remaining |= (pending && pre.dep[f] >= 0 ? 1u : 0u) << f;
         uint32_t spins = 0;
         while (__any_sync(FULL, pending)) {
             if (pending) {
                 const CellTable& t = *v.t;
-                bool ready = true;
+                uint32_t seen[6];
+#pragma unroll
+                for (int f = 0; f < 6; ++f) seen[f] = ((remaining >> f) & 1u) ? ld_relaxed_u32(&t.done[pre.dep[f]]) : 0u;
 #pragma unroll
                 for (int f = 0; f < 6; ++f)
-                    if (pre.dep[f] >= 0 && ld_acquire_u32(&t.done[pre.dep[f]]) != v.epoch) ready = false;
-                if (ready) {
+                    if (((remaining >> f) & 1u) && seen[f] == v.epoch) remaining &= ~(1u << f);
+                if (remaining == 0) {
+                    fence_acquire_gpu();
                     update_cell<MODE>(v, c, S, j, pre);
                     // release: this cell's field writes are visible before its done flag
                     st_release_u32(&t.done[j], v.epoch);
@@ -579,7 +583,8 @@ __global__ void __launch_bounds__(kTickThreads) k_surrogate_prepass(const __grid
         if (j < a.n) {
             CellPre pre;
             stage_cell(v, S, j, pre);
-            gather_transport(v, a.k, S, pre);
+            float4 nv[6][3];
+            gather_transport(v, a.k, S, pre, nv);
 #pragma unroll
             for (int k = 0; k < MARL_M_INT; ++k) xt[k * cap + j] = S.x[k][threadIdx.x];
             float f[mlp::kInPad];
@@ -654,6 +659,42 @@ constexpr int kCompactPerBlock = kCompactThreads * kCompactPerThread;
 
 __device__ __forceinline__ bool is_change(uint8_t e) { return e == MARL_EVENT_DIVISION || e == MARL_EVENT_DEATH; }
 
+// Change-list entries of the thread's flagged cells first + i (bit i of
+// `flags`), written from slot `pos` on (slots >= cap are dropped).  All loads
+// are issued before any store: the sources are scattered over the table, so
+// this costs one memory latency per thread instead of one per loaded value.
+__device__ __forceinline__ void write_changes(const CellTable& t, uint32_t first, uint32_t flags, uint32_t pos,
+                                              marl_change* __restrict__ out, uint32_t cap) {
+    float vals[kCompactPerThread][MARL_M_INT];
+    uint32_t st[kCompactPerThread];
+    uint8_t evs[kCompactPerThread];
+#pragma unroll
+    for (int i = 0; i < kCompactPerThread; ++i) {
+        if (!((flags >> i) & 1u)) continue;
+        const uint32_t j = first + i;
+        evs[i] = t.events[j];
+        st[i] = t.state[j];
+#pragma unroll
+        for (int k = 0; k < MARL_M_INT; ++k) vals[i][k] = __ldcg(&t.internal[(size_t)k * t.cap + j]);
+    }
+#pragma unroll
+    for (int i = 0; i < kCompactPerThread; ++i) {
+        if (!((flags >> i) & 1u)) continue;
+        if (pos < cap) {
+            marl_change& r = out[pos];
+            r.cell = first + i;
+            r.event = evs[i];
+            r.quiescent = (uint8_t)((st[i] >> 16) & 1u);
+            r._pad = 0;
+            // entries are 72 bytes, so internal[] is 8-byte aligned only
+#pragma unroll
+            for (int k = 0; k < MARL_M_INT; k += 2)
+                *reinterpret_cast<float2*>(&r.internal[k]) = make_float2(vals[i][k], vals[i][k + 1]);
+        }
+        ++pos;
+    }
+}
+
 __global__ void __launch_bounds__(kCompactThreads) k_count_events(const uint8_t* __restrict__ ev, uint32_t n,
                                                                   uint32_t* __restrict__ block_counts) {
     __shared__ uint32_t warp_sums[kCompactThreads / 32];
@@ -707,19 +748,8 @@ __global__ void __launch_bounds__(kCompactThreads) k_scatter_events(CellTable t,
     uint32_t warp_off = 0;
     for (int w = 0; w < warp; ++w) warp_off += warp_tot[w];
     uint32_t pos = block_off + warp_off + incl - cnt;
-    for (int i = 0; i < kCompactPerThread; ++i) {
-        if (!((flags >> i) & 1u)) continue;
-        const uint32_t j = first + i;
-        if (pos < cap) {
-            marl_change& r = out[pos];
-            r.cell = j;
-            r.event = t.events[j];
-            r.quiescent = (uint8_t)((t.state[j] >> 16) & 1u);
-            r._pad = 0;
-            for (int k = 0; k < MARL_M_INT; ++k) r.internal[k] = t.internal[(size_t)k * t.cap + j];
-        }
-        ++pos;
-    }
+    write_changes(t, first, flags, pos, out, cap);
+    pos += cnt;
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kCompactThreads - 1) {
         hdr->count = pos;
         hdr->n_cells = n;
@@ -758,20 +788,8 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact_batch(const RunDesc
             if (w < warp) warp_off += warp_tot[w];
             block_tot += warp_tot[w];
         }
-        uint32_t pos = s_off + warp_off + incl - cnt;
-        for (int i = 0; i < kCompactPerThread; ++i) {
-            if (!((flags >> i) & 1u)) continue;
-            const uint32_t j = first + i;
-            if (pos < R.change_cap) {
-                marl_change& c = R.changes[pos];
-                c.cell = j;
-                c.event = t.events[j];
-                c.quiescent = (uint8_t)((t.state[j] >> 16) & 1u);
-                c._pad = 0;
-                for (int k = 0; k < MARL_M_INT; ++k) c.internal[k] = t.internal[(size_t)k * t.cap + j];
-            }
-            ++pos;
-        }
+        const uint32_t pos = s_off + warp_off + incl - cnt;
+        write_changes(t, first, flags, pos, R.changes, R.change_cap);
         __syncthreads();
         if (threadIdx.x == 0) s_off += block_tot;
         __syncthreads();
@@ -805,72 +823,89 @@ __global__ void __launch_bounds__(256) k_pack_changes(const RunDesc* __restrict_
 }
 
 // ------------------------------------------------------------- edits -----
-__device__ void write_record(CellTable& t, uint32_t slot, const marl_cell& c) {
-    const size_t cap = t.cap;
-    t.pos[slot] = pack_pos(c.pos[0], c.pos[1], c.pos[2]);
-    t.age[slot] = c.age;
-    t.state[slot] = (uint32_t)c.prep_remaining | ((uint32_t)(c.quiescent ? 1 : 0) << 16) |
-                    ((uint32_t)c.starter_type << 24);
-    t.lineage[slot] = c.lineage_id;
-    for (int k = 0; k < MARL_M_INT; ++k) t.internal[k * cap + slot] = c.internal[k];
-    const marl_ruleset& r = c.ruleset;
-    uint32_t w[4] = {0, 0, 0, 0};
-    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
-        t.tp_rate[i * cap + slot] = make_float2(r.transport[i].uptake_rate, r.transport[i].secrete_rate);
-        w[i >> 1] |= ((uint32_t)r.transport[i].ext_species | ((uint32_t)r.transport[i].int_species << 8))
-                     << ((i & 1) * 16);
-    }
-    t.tp_idx[slot] = make_uint4(w[0], w[1], w[2], w[3]);
-    for (int i = 0; i < MARL_R_MAX; ++i) {
-        const marl_reaction& q = r.reactions[i];
-        const uint32_t idx = (uint32_t)q.substrate | ((uint32_t)q.product << 8) | ((uint32_t)q.catalyst << 16) |
-                             ((uint32_t)q.cofactor << 24);
-        t.rx[i * cap + slot] = make_uint4(idx, __float_as_uint(q.k_m), __float_as_uint(q.v_max), __float_as_uint(q.k_cat));
-    }
-    uint32_t e[4] = {0, 0, 0, 0};
-    for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
-        t.ef_par[i * cap + slot] = make_float2(r.effectors[i].threshold, r.effectors[i].rate);
-        e[i >> 1] |= ((uint32_t)r.effectors[i].int_species | ((uint32_t)r.effectors[i].ext_species << 8))
-                     << ((i & 1) * 16);
-    }
-    t.ef_idx[slot] = make_uint4(e[0], e[1], e[2], e[3]);
-    t.fate[slot] = make_float4(r.fate.division_energy, r.fate.death_energy, r.fate.quiescence_energy,
-                               r.fate.division_prep_ticks);
-    float* cold = t.cold + (size_t)slot * kColdFloats;
-    for (int i = 0; i < MARL_S_RECEPTORS; ++i) {
-        cold[3 * i] = r.receptors[i].k_half;
-        cold[3 * i + 1] = r.receptors[i].n_hill;
-        cold[3 * i + 2] = r.receptors[i].gain;
-    }
-    cold[24] = r.hgt_propensity;
-    cold[25] = r.mutation_rate;
-}
+// One warp per birth.  The warp copies the 656-byte record into shared
+// memory with 16-byte loads, then its lanes write the table's arrays in
+// parallel (lane r: reaction r and internal species r; lanes < 8: transporter
+// and effector rates; lanes < 26: cold floats; lanes 26-30: scalars).
+constexpr int kRecordU4 = (int)(sizeof(marl_cell) / 16);
+static_assert(sizeof(marl_cell) % 16 == 0, "cell records are whole 16-byte words");
+constexpr int kBirthWarps = 4;
 
-__device__ __forceinline__ void birth_one(CellTable t, const Grid g, int32_t* cmap, uint8_t* mask, uint32_t slot,
-                                          const marl_cell& c, uint32_t* err) {
+__device__ __forceinline__ void birth_warp(CellTable t, const Grid g, int32_t* cmap, uint8_t* mask, uint32_t slot,
+                                           const marl_cell* __restrict__ rec, uint4* stage, uint32_t* err) {
+    const int l = threadIdx.x & 31;
+    const uint4* src = reinterpret_cast<const uint4*>(rec);
+    for (int q = l; q < kRecordU4; q += 32) stage[q] = src[q];
+    __syncwarp();
+    const marl_cell& c = *reinterpret_cast<const marl_cell*>(stage);
     if (c.pos[0] >= g.X || c.pos[1] >= g.Y || c.pos[2] >= g.Z) {
-        atomicOr(err, kErrBadIndex);
+        if (l == 0) atomicOr(err, kErrBadIndex);
         return;
     }
-    write_record(t, slot, c);
-    const size_t row = (size_t)c.pos[2] * g.Y + c.pos[1];
-    cmap[row * g.X + c.pos[0]] = (int32_t)slot;
-    mask[row * mask_pitch(g.X) + c.pos[0]] = 1;
+    const size_t cap = t.cap;
+    const marl_ruleset& r = c.ruleset;
+    if (l < MARL_R_MAX) {
+        const marl_reaction& q = r.reactions[l];
+        const uint32_t idx = (uint32_t)q.substrate | ((uint32_t)q.product << 8) | ((uint32_t)q.catalyst << 16) |
+                             ((uint32_t)q.cofactor << 24);
+        t.rx[l * cap + slot] = make_uint4(idx, __float_as_uint(q.k_m), __float_as_uint(q.v_max), __float_as_uint(q.k_cat));
+        t.internal[l * cap + slot] = c.internal[l];
+    }
+    if (l < MARL_S_TRANSPORTERS) {
+        t.tp_rate[l * cap + slot] = make_float2(r.transport[l].uptake_rate, r.transport[l].secrete_rate);
+        t.ef_par[l * cap + slot] = make_float2(r.effectors[l].threshold, r.effectors[l].rate);
+    }
+    if (l < kColdFloats) {
+        const float v = l < 3 * MARL_S_RECEPTORS
+                            ? (l % 3 == 0 ? r.receptors[l / 3].k_half
+                                          : (l % 3 == 1 ? r.receptors[l / 3].n_hill : r.receptors[l / 3].gain))
+                            : (l == 24 ? r.hgt_propensity : r.mutation_rate);
+        t.cold[(size_t)slot * kColdFloats + l] = v;
+    }
+    if (l == 26) {
+        t.pos[slot] = pack_pos(c.pos[0], c.pos[1], c.pos[2]);
+        t.age[slot] = c.age;
+        const size_t row = (size_t)c.pos[2] * g.Y + c.pos[1];
+        cmap[row * g.X + c.pos[0]] = (int32_t)slot;
+        mask[row * mask_pitch(g.X) + c.pos[0]] = 1;
+    }
+    if (l == 27) {
+        t.state[slot] = (uint32_t)c.prep_remaining | ((uint32_t)(c.quiescent ? 1 : 0) << 16) |
+                        ((uint32_t)c.starter_type << 24);
+        t.lineage[slot] = c.lineage_id;
+    }
+    if (l == 28 || l == 29) {
+        uint32_t w[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t pair = l == 28 ? ((uint32_t)r.transport[i].ext_species | ((uint32_t)r.transport[i].int_species << 8))
+                                          : ((uint32_t)r.effectors[i].int_species | ((uint32_t)r.effectors[i].ext_species << 8));
+            w[i >> 1] |= pair << ((i & 1) * 16);
+        }
+        (l == 28 ? t.tp_idx : t.ef_idx)[slot] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    if (l == 30)
+        t.fate[slot] = make_float4(r.fate.division_energy, r.fate.death_energy, r.fate.quiescence_energy,
+                                   r.fate.division_prep_ticks);
 }
 
-__global__ void k_cells_from_records(const marl_cell* __restrict__ rec, uint32_t count, uint32_t base, CellTable t,
-                                     Grid g, int32_t* __restrict__ cmap, uint8_t* __restrict__ mask,
-                                     uint32_t* err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) birth_one(t, g, cmap, mask, base + i, rec[i], err);
+__global__ void __launch_bounds__(32 * kBirthWarps) k_cells_from_records(const marl_cell* __restrict__ rec,
+                                                                         uint32_t count, uint32_t base, CellTable t,
+                                                                         Grid g, int32_t* __restrict__ cmap,
+                                                                         uint8_t* __restrict__ mask, uint32_t* err) {
+    __shared__ uint4 stage[kBirthWarps][kRecordU4];
+    const uint32_t i = blockIdx.x * kBirthWarps + (threadIdx.x >> 5);
+    if (i < count) birth_warp(t, g, cmap, mask, base + i, rec + i, stage[threadIdx.x >> 5], err);
 }
 
-__global__ void k_births_batch(const RunDesc* __restrict__ runs, const marl_cell* __restrict__ recs,
-                               const uint2* __restrict__ slots, uint32_t count, uint32_t* err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * kBirthWarps) k_births_batch(const RunDesc* __restrict__ runs,
+                                                                   const marl_cell* __restrict__ recs,
+                                                                   const uint2* __restrict__ slots, uint32_t count,
+                                                                   uint32_t* err) {
+    __shared__ uint4 stage[kBirthWarps][kRecordU4];
+    const uint32_t i = blockIdx.x * kBirthWarps + (threadIdx.x >> 5);
     if (i >= count) return;
     const RunDesc& R = runs[slots[i].x];
-    birth_one(R.t, R.g, R.cmap, R.mask, slots[i].y, recs[i], err);
+    birth_warp(R.t, R.g, R.cmap, R.mask, slots[i].y, recs + i, stage[threadIdx.x >> 5], err);
 }
 
 __global__ void k_cells_to_records(CellTable t, uint32_t n, marl_cell* __restrict__ rec) {
@@ -1123,7 +1158,8 @@ cudaError_t launch_compact_events(const CellTable& t, uint32_t n, uint32_t* bloc
 cudaError_t launch_cells_from_records(const marl_cell* rec, uint32_t count, uint32_t base, CellTable t, const Grid& g,
                                       int32_t* cmap, uint8_t* mask, uint32_t* err, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    k_cells_from_records<<<blocks_for(count, 128), 128, 0, s>>>(rec, count, base, t, g, cmap, mask, err);
+    k_cells_from_records<<<blocks_for(count, kBirthWarps), 32 * kBirthWarps, 0, s>>>(rec, count, base, t, g, cmap,
+                                                                                      mask, err);
     return cudaGetLastError();
 }
 
@@ -1216,7 +1252,7 @@ cudaError_t launch_moves_batch(const RunDesc* runs, const uint4* items, uint32_t
 cudaError_t launch_births_batch(const RunDesc* runs, const marl_cell* recs, const uint2* slots, uint32_t count,
                                 uint32_t* err, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    k_births_batch<<<blocks_for(count, 128), 128, 0, s>>>(runs, recs, slots, count, err);
+    k_births_batch<<<blocks_for(count, kBirthWarps), 32 * kBirthWarps, 0, s>>>(runs, recs, slots, count, err);
     return cudaGetLastError();
 }
 
