@@ -389,6 +389,89 @@ def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int
     }
 
 
+def field_microbench_leg(marl, torch, stream, substeps: int = 100) -> dict:
+    """256x256x128 field microbenchmark: 100 diffusion substeps on device
+    buffers (marl_diffuse_device), then the Beer-Lambert scan."""
+    import workloads
+
+    dims = workloads.MICRO_DIMS
+    X, Y, Z = dims
+    field, occ = workloads.field_microbench()
+    p = marl.default_params()
+    f = torch.from_numpy(field).cuda()
+    scratch = torch.empty_like(f)
+    o = torch.from_numpy(occ).cuda()
+    marl.diffuse_device(f.data_ptr(), scratch.data_ptr(), o.data_ptr(), dims, p, 4, stream.cuda_stream)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    marl.diffuse_device(f.data_ptr(), scratch.data_ptr(), o.data_ptr(), dims, p, substeps, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    t_sub = e0.elapsed_time(e1) / 1000.0 / substeps
+    V = X * Y * Z
+    peak, src = peaks()
+    diff_gbs = BYTES_PER_VOXEL_SUBSTEP * V / t_sub / 1e9
+    # light: a context holding the diffused field (no cells)
+    ctx = marl.Context(dims, p, cell_capacity=1)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_field(f.cpu().numpy())
+    for _ in range(3):
+        ctx.light_update()
+    reps = 20
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.light_update()
+    e1.record(stream)
+    e1.synchronize()
+    t_light = e0.elapsed_time(e1) / 1000.0 / reps
+    ctx.close()
+    return {"workload": "256x256x128, 12 species U[0,1), 5% occupied as balls of radius 2-4, deposit factor "
+                        "U[0.5,1] through species 7, additive sources; 100 substeps, then the light scan "
+                        "(absorbance 0.05*U[0,1); the scan's context holds no cells)",
+            "us_per_substep": t_sub * 1e6, "diffusion_gbs_algorithmic": diff_gbs,
+            "diffusion_frac_of_measured_hbm": diff_gbs / peak, "bytes_per_voxel_substep": BYTES_PER_VOXEL_SUBSTEP,
+            "light_us": t_light * 1e6, "light_gbs_algorithmic": 9 * V / t_light / 1e9,
+            "light_frac_of_measured_hbm": 9 * V / t_light / 1e9 / peak, "peak_gbs": peak, "peak_source": src,
+            "l2": "the 384 MiB buffers exceed L2"}
+
+
+def cell_microbench_leg(marl, torch, stream, phases: int = 200) -> dict:
+    """1,000,000 cells on 256x256x128: 200 repetitions of the cell loop
+    (gather, transport, reactions, effectors, scatter) with no fate edits."""
+    import workloads
+
+    dims = workloads.MICRO_DIMS
+    field, _ = workloads.field_microbench()
+    cells = workloads.cell_microbench()
+    touched = workloads.touched_voxels(cells, dims)
+    p = marl.default_params()
+    ctx = marl.Context(dims, p, cell_capacity=len(cells))
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_field(field)
+    ctx.upload_cells(cells)
+    ctx.light_update()
+    lib = marl.load()
+    for _ in range(3):
+        marl._check(lib.marl_cell_phase(ctx.h, None), "marl_cell_phase")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(phases):
+        marl._check(lib.marl_cell_phase(ctx.h, None), "marl_cell_phase")
+    e1.record(stream)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1000.0 / phases
+    ctx.synchronize()
+    ctx.close()
+    alg = 592 * len(cells) + 96 * touched
+    peak, src = peaks()
+    return {"workload": "1,000,000 cells at unique random voxels of 256x256x128; 16 reactions with random "
+                        "wiring, v_max lognormal(0,1), k_m and k_cat U[0.01,1], light catalysis on 25%; "
+                        "8 transporters and 8 effectors; 200 cell-loop phases without fate edits",
+            "ms_per_phase": t * 1e3, "cells_per_s": len(cells) / t, "touched_empty_voxels": touched,
+            "algorithmic_bytes_per_phase": alg, "gbs_algorithmic": alg / t / 1e9,
+            "frac_of_measured_hbm": alg / t / 1e9 / peak, "peak_source": src}
+
+
 def peaks_bf16() -> float:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -409,6 +492,7 @@ def main() -> int:
     ap.add_argument("--no-roofline", action="store_true", help="skip the separate diffusion timing")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate leg")
+    ap.add_argument("--no-micro", action="store_true", help="skip the field and cell microbenchmarks")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -476,7 +560,10 @@ def main() -> int:
     roof = None
     if rank == 0 and not args.no_roofline:
         roof = diffusion_roofline(marl, torch, eng, stream, tuple(args.tile) if args.tile else None)
-    ens = surr = None
+    ens = surr = fmicro = cmicro = None
+    if rank == 0 and world == 1 and not args.no_micro:
+        fmicro = field_microbench_leg(marl, torch, stream)
+        cmicro = cell_microbench_leg(marl, torch, stream)
     if rank == 0 and world == 1 and not args.no_ensemble:
         ens = ensemble_leg(marl, torch, stream)
     if rank == 0 and world == 1 and not args.no_surrogate:
@@ -500,6 +587,8 @@ def main() -> int:
                     "api": "marl_engine_step (C ABI), wall clock per tick"},
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "field_microbench": fmicro,
+            "cell_microbench": cmicro,
             "ensemble": ens,
             "surrogate": surr,
         }
