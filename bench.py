@@ -244,38 +244,52 @@ ENSEMBLE_GRIDS = [(64, 64, 32), (96, 96, 48), (128, 128, 64), (128, 128, 96)]
 MLP_FLOP_PER_CELL = 2 * (93 * 256 + 256 * 256 + 256 * 16)  # algorithmic forward FLOPs (93 inputs)
 
 
-def ensemble_leg(marl, torch, stream, ticks: int = 30, warmup: int = 3) -> dict:
+def ensemble_leg(marl, torch, stream, ticks: int = 30, warmup: int = 3, surrogate=None) -> dict:
     """Batched ensemble: 64 runs (seeds 0-63), 16 each of four grid sizes, one
-    launch per phase for all runs, graph-captured device tick."""
-    runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
-    b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=1 << 16)
-    b.set_stream(stream.cuda_stream)
-    us = b.autotune(3)
-    b.step(warmup)
-    torch.cuda.synchronize()
-    c0 = b.counters()
-    t0 = time.perf_counter()
-    b.step(ticks)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    c1 = b.counters()
-    dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
-    pop = sum(b.stats(r)["population"] for r in range(len(runs)))
-    b.close()
-    return {"workload": "64 runs, seeds 0-63, 16 each of 64x64x32, 96x96x48, 128x128x64, 128x128x96; "
-                        f"ticks {warmup + 1}..{warmup + ticks}",
-            "run_ticks_per_s": len(runs) * ticks / dev_s, "e2e_run_ticks_per_s": len(runs) * ticks / wall,
-            "ms_per_batch_tick": 1000.0 * dev_s / ticks, "population_end": int(pop),
-            "autotune_us_per_batched_substep": us,
-            "note": "device time (CUDA events on the batch stream) of the graph-replayed device ticks and edit "
-                    "copies; e2e adds the host fate step of all runs on worker threads"}
+    launch per phase for all runs, graph-captured device tick; with a trained
+    surrogate, the same ticks again in the gated mode at 1e-3."""
+
+    def timed(mode):
+        runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
+        b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=1 << 16)
+        b.set_stream(stream.cuda_stream)
+        us = b.autotune(3)
+        if mode is not None:
+            b.set_surrogate(surrogate, mode, 1e-3)
+        b.step(warmup)
+        torch.cuda.synchronize()
+        c0 = b.counters()
+        t0 = time.perf_counter()
+        b.step(ticks)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        c1 = b.counters()
+        dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
+        pop = sum(b.stats(r)["population"] for r in range(len(runs)))
+        out = {"run_ticks_per_s": len(runs) * ticks / dev_s, "e2e_run_ticks_per_s": len(runs) * ticks / wall,
+               "ms_per_batch_tick": 1000.0 * dev_s / ticks, "population_end": int(pop),
+               "autotune_us_per_batched_substep": us}
+        if mode is not None:
+            out["surrogate_counters"] = {k: (float(v) if isinstance(v, float) else int(v))
+                                         for k, v in b.surrogate_counters().items()}
+        b.close()
+        return out
+
+    res = timed(None)
+    res["workload"] = ("64 runs, seeds 0-63, 16 each of 64x64x32, 96x96x48, 128x128x64, 128x128x96; "
+                       f"ticks {warmup + 1}..{warmup + ticks}")
+    res["note"] = ("device time (CUDA events on the batch stream) of the graph-replayed device ticks and edit "
+                   "copies; e2e adds the host fate step of all runs on worker threads")
+    if surrogate is not None:
+        res["with_surrogate_gated_1e-3"] = timed(marl.SURR_GATED)
+    return res
 
 
-def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int = 10_000_000) -> dict:
+def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int = 10_000_000):
     """Learned reaction surrogate: pairs captured from the plain cell kernel on
     seeded 128x128x64 default runs, trained on the GPU, evaluated on held-out
     rows and in the tick (gated at 1e-3 and trusted), against the plain tick
-    from the same state."""
+    from the same state.  Returns (trained surrogate, result)."""
     t_start = time.perf_counter()
     p = marl.default_params()
     s = marl.Surrogate(max_pairs=target_pairs, batch=8192, lr=2e-3, seed=5)
@@ -373,8 +387,7 @@ def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int
         err = np.abs(a - b).max(1) / np.maximum(np.abs(b).max(1), 1e-6)
         modes[name]["cell_phase_rel_err_max"] = float(err.max())
         modes[name]["cell_phase_cells_within_1e-3"] = float((err <= 1e-3).mean())
-    s.close()
-    return {
+    return s, {
         "workload": f"pairs from {seed - 100} seeded 128x128x64 default runs (ticks 21..<=600), "
                     f"{n} rows, last 5% held out; tick comparison from tick 400 of the seed-{SEED} run "
                     f"({len(cells)} cells)",
@@ -564,10 +577,13 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_micro:
         fmicro = field_microbench_leg(marl, torch, stream)
         cmicro = cell_microbench_leg(marl, torch, stream)
-    if rank == 0 and world == 1 and not args.no_ensemble:
-        ens = ensemble_leg(marl, torch, stream)
+    trained = None
     if rank == 0 and world == 1 and not args.no_surrogate:
-        surr = surrogate_leg(marl, torch, stream)
+        trained, surr = surrogate_leg(marl, torch, stream)
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        ens = ensemble_leg(marl, torch, stream, surrogate=trained)
+    if trained is not None:
+        trained.close()
     if rank == 0:
         base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline()
         line = {

@@ -506,6 +506,13 @@ marl_status marl_surrogate_infer_device(marl_surrogate* s, const uint16_t* x_dev
  * gated mode.  The surrogate must outlive its use by the context. */
 marl_status marl_ctx_set_surrogate(marl_ctx* ctx, marl_surrogate* s, int32_t mode, float tol);
 marl_status marl_ctx_surrogate_counters(marl_ctx* ctx, marl_surrogate_counters* out);
+/* The same for every run of a batch (modes OFF, GATED, TRUSTED): one
+ * pre-pass over all runs' cells and one inference over all of them per tick.
+ * While a surrogate is attached the device tick is launched directly rather
+ * than replayed from the captured graph (the inference's row count changes
+ * every tick). */
+marl_status marl_batch_set_surrogate(marl_batch* b, marl_surrogate* s, int32_t mode, float tol);
+marl_status marl_batch_surrogate_counters(marl_batch* b, marl_surrogate_counters* out);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,7 @@
 #include "ctx_impl.h"
 #include "engine_host.h"
 #include "internal.h"
+#include "surrogate.h"
 
 namespace marl {
 namespace {
@@ -167,6 +168,19 @@ struct marl_batch {
     marl_cell* h_records = nullptr;
     uint32_t records_cap = 0;
 
+    // Reaction surrogate (marl_batch_set_surrogate); its arrays hold one row
+    // per cell slot of the batch, run r's cells from the run's cell_base.
+    marl_surrogate* surr = nullptr;
+    int surr_mode = MARL_SURR_OFF;
+    float surr_tol = 0.0f;
+    uint32_t surr_rows = 0;  // sum of the runs' capacities
+    float* surr_xt = nullptr;
+    float* surr_pred = nullptr;
+    void* surr_x = nullptr;
+    uint8_t* surr_status = nullptr;
+    float* surr_err = nullptr;
+    unsigned long long* surr_counters = nullptr;
+
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool use_graph = true;
     bool direct_since_change = false;  // a direct tick ran since the last graph invalidation
@@ -216,7 +230,8 @@ void batch_free(marl_batch* b) {
             if (q) cudaFree(q);
         free_table(r.t);
     }
-    void* dev[] = {b->d_runs, b->d_maps, b->d_diff_items, b->d_light_items, b->d_rb, b->d_edit, b->d_records};
+    void* dev[] = {b->d_runs, b->d_maps, b->d_diff_items, b->d_light_items, b->d_rb, b->d_edit, b->d_records,
+                   b->surr_xt, b->surr_pred, b->surr_x, b->surr_status, b->surr_err, b->surr_counters};
     for (void* p : dev)
         if (p) cudaFree(p);
     void* host[] = {b->h_runs, b->h_rb, b->h_edit, b->h_records};
@@ -337,8 +352,29 @@ void fill_desc(marl_batch* b) {
         d.n = R.n;
         d.epoch = b->epoch;
         d.cell_base = base;
+        d.sv = SurrView{};
+        if (b->surr) {
+            d.sv.xt = b->surr_xt;
+            d.sv.pred = b->surr_pred;
+            d.sv.tol = b->surr_tol;
+            d.sv.status = b->surr_status;
+            d.sv.err = b->surr_err;
+            d.sv.row0 = base;
+            d.sv.ld = b->surr_rows;
+        }
         base += R.n;
     }
+}
+
+uint32_t batch_cells(const marl_batch* b) {
+    uint32_t n = 0;
+    for (const auto& R : b->runs) n += R.n;
+    return n;
+}
+
+int surrogate_cell_mode(const marl_batch* b) {
+    if (!b->surr) return kModePlain;
+    return b->surr_mode == MARL_SURR_TRUSTED ? kModeTrusted : kModeGated;
 }
 
 // The device part of one tick (crates/marl-sim/src/lib.rs:164-217 for every
@@ -361,7 +397,20 @@ marl_status enqueue_device_tick(marl_batch* b, cudaStream_t s, int cur) {
         cur ^= 1;
     }
     CK(launch_light_batch(b->d_runs, b->d_light_items, b->n_light_items, b->fk, cur, S > 0 ? 1 : 0, s));
-    CK(launch_cell_tick_batch(b->d_runs, n_runs, b->d_scalars(), b->ck, cur, b->num_sms, s));
+    const int mode = surrogate_cell_mode(b);
+    const uint32_t total = batch_cells(b);
+    if (mode != kModePlain && total > 0) {
+        // Launched directly, never captured: the row count changes every tick.
+        CK(launch_surrogate_prepass_batch(b->d_runs, n_runs, total, b->ck, cur, b->surr->norm, b->surr_xt,
+                                          b->surr_rows, b->surr_x, b->num_sms, s));
+        marl_status st = surrogate_infer(b->surr, reinterpret_cast<const __nv_bfloat16*>(b->surr_x), total,
+                                         b->surr_pred, b->surr_rows, s);
+        if (st) return st;
+    }
+    CK(launch_cell_tick_batch(b->d_runs, n_runs, b->d_scalars(), b->ck, cur, b->num_sms, mode, s));
+    if (mode != kModePlain && total > 0)
+        CK(launch_surrogate_count(b->surr_status, b->surr_err, total, b->surr_counters,
+                                  reinterpret_cast<uint32_t*>(b->surr_counters + 4), s));
     CK(launch_compact_batch(b->d_runs, n_runs, s));
     CK(launch_pack_changes(b->d_runs, n_runs, b->d_scalars(), b->d_packed(), s));
     CK(cudaMemcpyAsync(b->h_rb, b->d_rb, b->rb_head_bytes, cudaMemcpyDeviceToHost, s));
@@ -370,12 +419,12 @@ marl_status enqueue_device_tick(marl_batch* b, cudaStream_t s, int cur) {
 
 uint64_t device_tick_launches(const marl_batch* b) {
     const uint32_t S = b->sim.diffusion_substeps;
-    return 1 + (S ? S : b->runs.size()) + 4;
+    return 1 + (S ? S : b->runs.size()) + 4 + (b->surr ? 5 : 0);
 }
 
 marl_status launch_tick(marl_batch* b) {
     const int cur = b->cur;
-    if (b->use_graph && b->direct_since_change) {
+    if (b->use_graph && b->direct_since_change && !b->surr) {
         if (!b->graph[cur]) {
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
@@ -755,6 +804,50 @@ marl_status marl_batch_autotune(marl_batch* b, int32_t reps, float* best_us_out)
 marl_status marl_batch_set_graph(marl_batch* b, int32_t use_graph) {
     if (!b) return fail(MARL_ERR_INVALID_INPUT, "null batch");
     b->use_graph = use_graph != 0;
+    return MARL_OK;
+}
+
+marl_status marl_batch_set_surrogate(marl_batch* b, marl_surrogate* s, int32_t mode, float tol) {
+    if (!b) return fail(MARL_ERR_INVALID_INPUT, "null batch");
+    if (mode != MARL_SURR_OFF && mode != MARL_SURR_GATED && mode != MARL_SURR_TRUSTED)
+        return fail(MARL_ERR_INVALID_INPUT, "batch surrogate mode must be OFF, GATED or TRUSTED");
+    if (mode != MARL_SURR_OFF && (!s || !s->prepared))
+        return fail(MARL_ERR_STATE, "surrogate missing or not prepared");
+    if (mode == MARL_SURR_GATED && !(tol >= 0.0f)) return fail(MARL_ERR_INVALID_INPUT, "tol must be >= 0");
+    CK(cudaStreamSynchronize(b->stream));
+    if (mode != MARL_SURR_OFF && !b->surr_xt) {
+        uint64_t rows = 0;
+        for (const auto& R : b->runs) rows += R.cap;
+        if (rows > 0xFFFFFFFFull) return fail(MARL_ERR_CAPACITY, "batch capacity exceeds 2^32 cells");
+        b->surr_rows = (uint32_t)rows;
+        CK(cudaMalloc((void**)&b->surr_xt, rows * MARL_M_INT * 4));
+        CK(cudaMalloc((void**)&b->surr_pred, rows * MARL_M_INT * 4));
+        CK(cudaMalloc((void**)&b->surr_x, rows * mlp::kInPad * 2));
+        CK(cudaMalloc((void**)&b->surr_status, rows));
+        CK(cudaMalloc((void**)&b->surr_err, rows * 4));
+        CK(cudaMalloc((void**)&b->surr_counters, 64));
+        CK(cudaMemset(b->surr_counters, 0, 64));
+    }
+    b->surr = mode == MARL_SURR_OFF ? nullptr : s;
+    b->surr_mode = mode;
+    b->surr_tol = tol;
+    invalidate_graphs(b);
+    return MARL_OK;
+}
+
+marl_status marl_batch_surrogate_counters(marl_batch* b, marl_surrogate_counters* out) {
+    if (!b || !out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    CK(cudaStreamSynchronize(b->stream));
+    if (!b->surr_counters) return MARL_OK;
+    unsigned long long h[8];
+    CK(cudaMemcpy(h, b->surr_counters, 64, cudaMemcpyDeviceToHost));
+    out->cells = h[0];
+    out->speculated = h[1];
+    out->accepted = h[2];
+    out->rejected = h[3];
+    const uint32_t bits = (uint32_t)h[4];
+    std::memcpy(&out->max_err, &bits, 4);
     return MARL_OK;
 }
 

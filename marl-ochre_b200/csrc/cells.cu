@@ -358,18 +358,19 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
         }
     } else {
         const SurrView& sv = *v.sv;
-        const size_t cap = t.cap;
+        const size_t ld = sv.ld;
+        const size_t row = sv.row0 + j;
         bool spec = true;
 #pragma unroll
         for (int k = 0; k < MARL_M_INT; ++k)
-            spec = spec && __float_as_uint(S.x[k][tid]) == __float_as_uint(sv.xt[k * cap + j]);
+            spec = spec && __float_as_uint(S.x[k][tid]) == __float_as_uint(sv.xt[k * ld + row]);
         uint8_t status = kSurrNotSpeculated;
         float err = 0.0f;
         if (MODE == kModeTrusted && spec) {
             active = active_reactions(c, S);
 #pragma unroll
             for (int k = 0; k < MARL_M_INT; ++k)
-                S.x[k][tid] = fminf(fmaxf(S.x[k][tid] + sv.pred[k * cap + j], 0.0f), c.c_max);
+                S.x[k][tid] = fminf(fmaxf(S.x[k][tid] + sv.pred[k * ld + row], 0.0f), c.c_max);
             status = kSurrAccepted;
         } else {
             active = reactions(c, S);
@@ -379,7 +380,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
                 float num = 0.0f, den = 0.0f;
 #pragma unroll
                 for (int k = 0; k < MARL_M_INT; ++k) {
-                    const float xs = fminf(fmaxf(sv.xt[k * cap + j] + sv.pred[k * cap + j], 0.0f), c.c_max);
+                    const float xs = fminf(fmaxf(sv.xt[k * ld + row] + sv.pred[k * ld + row], 0.0f), c.c_max);
                     num = fmaxf(num, fabsf(xs - S.x[k][tid]));
                     den = fmaxf(den, fabsf(S.x[k][tid]));
                 }
@@ -387,15 +388,15 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
                 if (err <= sv.tol) {
 #pragma unroll
                     for (int k = 0; k < MARL_M_INT; ++k)
-                        S.x[k][tid] = fminf(fmaxf(sv.xt[k * cap + j] + sv.pred[k * cap + j], 0.0f), c.c_max);
+                        S.x[k][tid] = fminf(fmaxf(sv.xt[k * ld + row] + sv.pred[k * ld + row], 0.0f), c.c_max);
                     status = kSurrAccepted;
                 } else {
                     status = kSurrRejected;
                 }
             }
         }
-        sv.status[j] = status;
-        sv.err[j] = err;
+        sv.status[row] = status;
+        sv.err[row] = err;
     }
 
     // Maintenance (cell.rs:291-311)
@@ -567,6 +568,36 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constan
     });
 }
 
+// One cell of the surrogate pre-pass: gather and transport of cell j from the
+// current field, its post-transport state into row `row` of xt [16][ld], and
+// its standardised BF16 features into row `row` of X [.][128].
+__device__ __forceinline__ void prepass_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
+                                             uint32_t row, size_t ld, const float* __restrict__ norm,
+                                             float* __restrict__ xt, __nv_bfloat16* __restrict__ X) {
+    CellPre pre;
+    stage_cell(v, S, j, pre);
+    float4 nv[6][3];
+    gather_transport(v, c, S, pre, nv);
+#pragma unroll
+    for (int k = 0; k < MARL_M_INT; ++k) xt[k * ld + row] = S.x[k][threadIdx.x];
+    float f[mlp::kInPad];
+#pragma unroll
+    for (int i = mlp::kIn; i < mlp::kInPad; ++i) f[i] = 0.0f;
+    surrogate_features(S, pre.light, [&](int i, float val) {
+        f[i] = (mlp::feature_transform(i, val) - norm[i]) / norm[mlp::kIn + i];
+    });
+    uint4* dst = reinterpret_cast<uint4*>(X + (size_t)row * mlp::kInPad);
+#pragma unroll
+    for (int q = 0; q < mlp::kInPad / 8; ++q) {
+        __nv_bfloat162 h0 = __floats2bfloat162_rn(f[8 * q], f[8 * q + 1]);
+        __nv_bfloat162 h1 = __floats2bfloat162_rn(f[8 * q + 2], f[8 * q + 3]);
+        __nv_bfloat162 h2 = __floats2bfloat162_rn(f[8 * q + 4], f[8 * q + 5]);
+        __nv_bfloat162 h3 = __floats2bfloat162_rn(f[8 * q + 6], f[8 * q + 7]);
+        dst[q] = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
+                            *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
+    }
+}
+
 // Surrogate pre-pass: gather_transport of every cell on the tick's starting
 // field, with no dependency waits.  A cell none of whose neighbour voxels is
 // written by an earlier cell gets exactly the state the cell loop will see.
@@ -577,32 +608,26 @@ __global__ void __launch_bounds__(kTickThreads) k_surrogate_prepass(const __grid
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const CellRunView v{&a.t, a.g, a.field, a.light, a.epoch, nullptr};
-    const size_t cap = a.t.cap;
     for (uint32_t base = blockIdx.x * kTickThreads; base < a.n; base += gridDim.x * kTickThreads) {
         const uint32_t j = base + threadIdx.x;
-        if (j < a.n) {
-            CellPre pre;
-            stage_cell(v, S, j, pre);
-            float4 nv[6][3];
-            gather_transport(v, a.k, S, pre, nv);
-#pragma unroll
-            for (int k = 0; k < MARL_M_INT; ++k) xt[k * cap + j] = S.x[k][threadIdx.x];
-            float f[mlp::kInPad];
-#pragma unroll
-            for (int i = mlp::kIn; i < mlp::kInPad; ++i) f[i] = 0.0f;
-            surrogate_features(S, pre.light, [&](int i, float val) {
-                f[i] = (mlp::feature_transform(i, val) - norm[i]) / norm[mlp::kIn + i];
-            });
-            uint4* row = reinterpret_cast<uint4*>(X + (size_t)j * mlp::kInPad);
-#pragma unroll
-            for (int q = 0; q < mlp::kInPad / 8; ++q) {
-                __nv_bfloat162 h0 = __floats2bfloat162_rn(f[8 * q], f[8 * q + 1]);
-                __nv_bfloat162 h1 = __floats2bfloat162_rn(f[8 * q + 2], f[8 * q + 3]);
-                __nv_bfloat162 h2 = __floats2bfloat162_rn(f[8 * q + 4], f[8 * q + 5]);
-                __nv_bfloat162 h3 = __floats2bfloat162_rn(f[8 * q + 6], f[8 * q + 7]);
-                row[q] = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
-                                    *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
-            }
+        if (j < a.n) prepass_cell(v, a.k, S, j, j, a.t.cap, norm, xt, X);
+    }
+}
+
+// Batched form: global row gi = cell_base(run) + j.
+__global__ void __launch_bounds__(kTickThreads) k_surrogate_prepass_batch(const RunDesc* __restrict__ runs, int n_runs,
+                                                                         uint32_t total, CellConsts c, int parity,
+                                                                         const float* __restrict__ norm,
+                                                                         float* __restrict__ xt, uint32_t ld,
+                                                                         __nv_bfloat16* __restrict__ X) {
+    extern __shared__ __align__(16) unsigned char tick_smem[];
+    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
+    for (uint32_t base = blockIdx.x * kTickThreads; base < total; base += gridDim.x * kTickThreads) {
+        const uint32_t gi = base + threadIdx.x;
+        if (gi < total) {
+            const RunDesc& R = runs[find_run(runs, n_runs, gi)];
+            const CellRunView v{&R.t, R.g, R.field[parity], R.light, R.epoch, nullptr};
+            prepass_cell(v, c, S, gi - R.cell_base, gi, ld, norm, xt, X);
         }
     }
 }
@@ -640,14 +665,15 @@ __global__ void k_surrogate_count(const uint8_t* __restrict__ status, const floa
 // Batched form: tickets run over the cells of all runs, run-major (run r's
 // cell j is ticket cell_base(r) + j), so every dependency of a cell, which lies
 // in the same run at a smaller index, also has a smaller ticket.
+template <int MODE>
 __global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc* __restrict__ runs, int n_runs,
                                                                   BatchScalars* __restrict__ bs, CellConsts c,
                                                                   int parity) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    cell_tick_loop<kModePlain>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    cell_tick_loop<MODE>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         const RunDesc& R = runs[find_run(runs, n_runs, gi)];
-        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, nullptr};
+        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv};
         j = gi - R.cell_base;
     });
 }
@@ -1137,6 +1163,26 @@ cudaError_t launch_surrogate_prepass(const CellLaunch& a, const float* norm, flo
     return cudaGetLastError();
 }
 
+cudaError_t launch_surrogate_prepass_batch(const RunDesc* runs, int n_runs, uint32_t total, const CellConsts& k,
+                                           int parity, const float* norm, float* xt, uint32_t ld, void* X,
+                                           int num_sms, cudaStream_t s) {
+    if (total == 0) return cudaSuccess;
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e =
+            cudaFuncSetAttribute(k_surrogate_prepass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    const uint32_t blocks_needed = (total + kTickThreads - 1) / kTickThreads;
+    const uint32_t cap_blocks = (uint32_t)num_sms * 8u;
+    k_surrogate_prepass_batch<<<blocks_needed < cap_blocks ? blocks_needed : cap_blocks, kTickThreads, kTickSmem, s>>>(
+        runs, n_runs, total, k, parity, norm, xt, ld, reinterpret_cast<__nv_bfloat16*>(X));
+    return cudaGetLastError();
+}
+
 cudaError_t launch_surrogate_count(const uint8_t* status, const float* err, uint32_t n,
                                    unsigned long long* counters, uint32_t* max_bits, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
@@ -1201,23 +1247,34 @@ cudaError_t launch_cell_schedule_batch(const RunDesc* runs, int n_runs, int num_
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_tick_batch(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k, int parity,
-                                   int num_sms, cudaStream_t s) {
+template <int MODE>
+static cudaError_t launch_cell_tick_batch_mode(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k,
+                                               int parity, int num_sms, cudaStream_t s) {
     static int per_sm = 0, configured_device = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_device != dev) {
         cudaError_t e =
-            cudaFuncSetAttribute(k_cell_tick_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+            cudaFuncSetAttribute(k_cell_tick_batch<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick_batch, kTickThreads, kTickSmem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick_batch<MODE>, kTickThreads, kTickSmem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         configured_device = dev;
     }
     // Persistent over all resident slots; the cell count is read on the device.
-    k_cell_tick_batch<<<per_sm * num_sms, kTickThreads, kTickSmem, s>>>(runs, n_runs, bs, k, parity);
+    k_cell_tick_batch<MODE><<<per_sm * num_sms, kTickThreads, kTickSmem, s>>>(runs, n_runs, bs, k, parity);
     return cudaGetLastError();
+}
+
+cudaError_t launch_cell_tick_batch(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k, int parity,
+                                   int num_sms, int mode, cudaStream_t s) {
+    switch (mode) {
+        case kModePlain: return launch_cell_tick_batch_mode<kModePlain>(runs, n_runs, bs, k, parity, num_sms, s);
+        case kModeGated: return launch_cell_tick_batch_mode<kModeGated>(runs, n_runs, bs, k, parity, num_sms, s);
+        case kModeTrusted: return launch_cell_tick_batch_mode<kModeTrusted>(runs, n_runs, bs, k, parity, num_sms, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_compact_batch(const RunDesc* runs, int n_runs, cudaStream_t s) {

@@ -267,6 +267,8 @@ marl_status enqueue_cell_phase(marl_ctx* c) {
         a.sv.tol = c->surr_tol;
         a.sv.status = c->surr_status;
         a.sv.err = c->surr_err;
+        a.sv.row0 = 0;
+        a.sv.ld = c->t.cap;
     }
     CK(launch_cell_tick(a, c->num_sms, c->stream));
     ++c->launches;

@@ -50,6 +50,29 @@ struct ChangeHeader {  // device-written, read back with the change list
 };
 static_assert(sizeof(ChangeHeader) == 64, "change header is 64 bytes");
 
+// Surrogate hooks of the cell loop (modes of k_cell_tick).
+constexpr int kModePlain = 0;
+constexpr int kModeCapture = 1;   // plain, and each cell writes its raw training row
+constexpr int kModeGated = 2;     // prediction checked against the plain reaction phase
+constexpr int kModeTrusted = 3;   // prediction taken unchecked where speculation holds
+constexpr uint8_t kSurrNotSpeculated = 0;
+constexpr uint8_t kSurrAccepted = 1;
+constexpr uint8_t kSurrRejected = 2;
+
+// Cell j of a run is row row0 + j of the surrogate arrays; species k of a
+// row is at k * ld + row.
+struct SurrView {
+    float* raw = nullptr;        // capture: row j (MARL_SURR_RAW_STRIDE floats) for cell j
+    uint32_t raw_rows = 0;       // capture: cells j < raw_rows write a row
+    const float* xt = nullptr;   // [16][ld] post-transport state from the pre-pass
+    const float* pred = nullptr; // [16][ld] predicted reaction deltas
+    float tol = 0.0f;
+    uint8_t* status = nullptr;   // [ld] kSurr*
+    float* err = nullptr;        // [ld] normwise error of the prediction (gated mode)
+    uint32_t row0 = 0;
+    uint32_t ld = 0;
+};
+
 // One run of a batch, as the batched kernels see it (device memory).
 struct RunDesc {
     Grid g;
@@ -67,6 +90,7 @@ struct RunDesc {
     marl_change* changes;
     uint32_t change_cap;
     uint32_t pad2;
+    SurrView sv;  // surrogate arrays of the batch, rows from cell_base
 };
 // Tensor maps per run in the batch's map array: load from buffer 0 / 1,
 // store into buffer 0 / 1, occupancy mask.
@@ -89,8 +113,14 @@ cudaError_t launch_diffuse_batch(int tile, const RunDesc* runs, const CUtensorMa
 cudaError_t launch_light_batch(const RunDesc* runs, const int4* items, int n_items, const FieldConsts& k, int parity,
                                int use_c4, cudaStream_t s);
 cudaError_t launch_cell_schedule_batch(const RunDesc* runs, int n_runs, int num_sms, cudaStream_t s);
+// mode: kModePlain, kModeGated or kModeTrusted (the runs' sv hold the arrays).
 cudaError_t launch_cell_tick_batch(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k, int parity,
-                                   int num_sms, cudaStream_t s);
+                                   int num_sms, int mode, cudaStream_t s);
+// Surrogate pre-pass over the first `total` cells of the batch (global rows):
+// xt [16][ld] and standardised BF16 features X [rows][128].
+cudaError_t launch_surrogate_prepass_batch(const RunDesc* runs, int n_runs, uint32_t total, const CellConsts& k,
+                                           int parity, const float* norm, float* xt, uint32_t ld, void* X,
+                                           int num_sms, cudaStream_t s);
 cudaError_t launch_compact_batch(const RunDesc* runs, int n_runs, cudaStream_t s);
 // Concatenates the runs' change lists in run order into `packed` (run r's
 // entries start at the sum of the counts of runs < r) and stores the total
@@ -103,25 +133,6 @@ cudaError_t launch_clear_dead_batch(const RunDesc* runs, const uint2* items, uin
 cudaError_t launch_moves_batch(const RunDesc* runs, const uint4* items, uint32_t count, cudaStream_t s);
 cudaError_t launch_births_batch(const RunDesc* runs, const marl_cell* recs, const uint2* slots, uint32_t count,
                                 uint32_t* err, cudaStream_t s);
-
-// Surrogate hooks of the cell loop (modes of k_cell_tick).
-constexpr int kModePlain = 0;
-constexpr int kModeCapture = 1;   // plain, and each cell writes its raw training row
-constexpr int kModeGated = 2;     // prediction checked against the plain reaction phase
-constexpr int kModeTrusted = 3;   // prediction taken unchecked where speculation holds
-constexpr uint8_t kSurrNotSpeculated = 0;
-constexpr uint8_t kSurrAccepted = 1;
-constexpr uint8_t kSurrRejected = 2;
-
-struct SurrView {
-    float* raw = nullptr;        // capture: row j (MARL_SURR_RAW_STRIDE floats) for cell j
-    uint32_t raw_rows = 0;       // capture: cells j < raw_rows write a row
-    const float* xt = nullptr;   // [16][cap] post-transport state from the pre-pass
-    const float* pred = nullptr; // [16][cap] predicted reaction deltas
-    float tol = 0.0f;
-    uint8_t* status = nullptr;   // [cap] kSurr*
-    float* err = nullptr;        // [cap] normwise error of the prediction (gated mode)
-};
 
 struct CellLaunch {
     int mode = kModePlain;

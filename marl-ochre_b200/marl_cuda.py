@@ -179,6 +179,7 @@ EXPORTED = [
     "marl_surrogate_prepare", "marl_surrogate_set_lr", "marl_surrogate_train", "marl_surrogate_evaluate",
     "marl_surrogate_get_weights", "marl_surrogate_set_weights", "marl_surrogate_gradients",
     "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
+    "marl_batch_set_surrogate", "marl_batch_surrogate_counters",
 ]
 
 _lib = None
@@ -270,6 +271,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_surrogate_infer_device": (c_int32, [P, P, c_uint32, P, c_uint32]),
         "marl_ctx_set_surrogate": (c_int32, [P, P, c_int32, c_float]),
         "marl_ctx_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
+        "marl_batch_set_surrogate": (c_int32, [P, P, c_int32, c_float]),
+        "marl_batch_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -650,6 +653,15 @@ class Batch:
 
     def step(self, ticks: int = 1) -> None:
         _check(self.lib.marl_batch_step(self.h, ticks), "marl_batch_step")
+
+    def set_surrogate(self, surrogate: "Surrogate | None", mode: int, tol: float = 1e-3) -> None:
+        _check(self.lib.marl_batch_set_surrogate(self.h, surrogate.h if surrogate is not None else None, mode, tol),
+               "marl_batch_set_surrogate")
+
+    def surrogate_counters(self) -> dict:
+        c = SurrogateCounters()
+        _check(self.lib.marl_batch_surrogate_counters(self.h, ctypes.byref(c)), "marl_batch_surrogate_counters")
+        return {name: getattr(c, name) for name, _ in SurrogateCounters._fields_}
 
     def counters(self) -> dict:
         c = Counters()

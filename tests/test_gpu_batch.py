@@ -82,3 +82,55 @@ def test_batch_errors(marl):
         b.set_tile(99, 16)
     b.step(2)
     assert b.stats(0)["tick"] == 2
+
+
+def captured_surrogate(marl, p, seed=3):
+    """A surrogate standardised on pairs captured from one single-run engine
+    (untrained weights: the modes' bookkeeping does not need a good network)."""
+    e = marl.Engine((32, 24, 24), p, rng_seed=seed, seed_count=30, cell_capacity=1 << 14)
+    s = marl.Surrogate(max_pairs=200_000, batch=128, seed=seed)
+    e.step(10)
+    marl.ctx_set_surrogate(e.lib.marl_engine_ctx(e.h), s, marl.SURR_CAPTURE)
+    e.step(15)
+    marl.ctx_set_surrogate(e.lib.marl_engine_ctx(e.h), None, marl.SURR_OFF)
+    s.prepare(s.pair_count())
+    return s
+
+
+def test_batch_surrogate_gated_zero_tolerance_is_plain(marl):
+    """The batched surrogate path at tolerance 0 reproduces the plain batch bit
+    for bit (a prediction is kept only when it equals the plain result)."""
+    p = marl.default_params()
+    runs = RUNS[:3]
+    s = captured_surrogate(marl, p)
+    plain = marl.Batch(runs, p, cell_capacity=1 << 14)
+    plain.step(30)
+    gated = marl.Batch(runs, p, cell_capacity=1 << 14)
+    gated.step(5)
+    gated.set_surrogate(s, marl.SURR_GATED, 0.0)
+    gated.step(25)
+    c = gated.surrogate_counters()
+    assert c["cells"] > 0 and c["accepted"] + c["rejected"] == c["speculated"] <= c["cells"]
+    assert c["max_err"] == 0.0
+    for r in range(len(runs)):
+        assert plain.cells(r).tobytes() == gated.cells(r).tobytes(), r
+        assert np.array_equal(plain.field(r).view(np.uint32), gated.field(r).view(np.uint32)), r
+    gated.set_surrogate(None, marl.SURR_OFF)
+    gated.step(2)  # back to the captured-graph plain tick
+    s.close()
+
+
+def test_batch_surrogate_trusted_runs(marl):
+    p = marl.default_params()
+    s = captured_surrogate(marl, p, seed=8)
+    b = marl.Batch(RUNS, p, cell_capacity=1 << 14)
+    b.set_surrogate(s, marl.SURR_TRUSTED)
+    b.step(20)
+    c = b.surrogate_counters()
+    assert c["rejected"] == 0 and c["accepted"] == c["speculated"] > 0
+    for r in range(len(RUNS)):
+        x = b.cells(r)["internal"]
+        assert np.all(np.isfinite(x)) and np.all(x >= 0)
+    with pytest.raises(marl.MarlError):
+        b.set_surrogate(s, marl.SURR_CAPTURE)
+    s.close()
