@@ -215,6 +215,7 @@ CellLaunch cell_launch(marl_ctx* c) {
 marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources, bool emit_c4 = false,
                             bool* c4_written = nullptr) {
     if (c4_written) *c4_written = false;
+    if (substeps > 0) c->c4_valid = false;
     if (substeps == 0) {
         if (fuse_sources) {
             CK(launch_sources(c->field[c->cur], c->g, c->fk, c->stream));
@@ -228,6 +229,7 @@ marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources, b
                           c->stream));
         c->cur ^= 1;
         ++c->launches;
+        if (c4) c->c4_valid = true;
         if (c4 && c4_written) *c4_written = true;
     }
     return MARL_OK;
@@ -235,6 +237,7 @@ marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources, b
 
 marl_status enqueue_cell_phase(marl_ctx* c) {
     if (c->n == 0) return MARL_OK;
+    c->c4_valid = false;  // the scatter writes every species
     CellLaunch a = cell_launch(c);
     if (c->schedule_dirty) {
         CK(launch_cell_schedule(a, c->stream));
@@ -562,6 +565,7 @@ marl_status marl_ctx_autotune(marl_ctx* c, int32_t reps, float* best_us_out) {
 
 marl_status marl_upload_field(marl_ctx* c, const float* f) {
     if (!c || !f) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    c->c4_valid = false;
     CK(cudaMemcpyAsync(c->field[c->cur], f, c->g.V() * 48, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return MARL_OK;
@@ -654,12 +658,13 @@ marl_status marl_diffuse(marl_ctx* c, uint32_t substeps, int32_t fuse_sources) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
     if (substeps > 0 && c->sim.diffusion_substeps == 0)
         return fail(MARL_ERR_INVALID_INPUT, "sim.diffusion_substeps == 0 gives no dt_sub");
-    return enqueue_diffuse(c, substeps, fuse_sources != 0);
+    // The last substep also writes species 4 compactly for a following light scan.
+    return enqueue_diffuse(c, substeps, fuse_sources != 0, true);
 }
 
 marl_status marl_light_update(marl_ctx* c) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
-    CK(launch_light(nullptr, c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
+    CK(launch_light(c->c4_valid ? c->c4 : nullptr, c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
     ++c->launches;
     return MARL_OK;
 }
@@ -784,6 +789,7 @@ marl_status marl_mass_f64(marl_ctx* c, double out[MARL_S_EXT]) {
 }
 
 marl_status marl_diffuse_tick_with_cells(marl_ctx* c, float* field, const uint8_t* occupancy) {
+    if (c) c->c4_valid = false;
     if (!c || !field || !occupancy) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     if (c->sim.diffusion_substeps == 0) return MARL_OK;  // field_diffusion.rs:176-178
     const size_t V = c->g.V();

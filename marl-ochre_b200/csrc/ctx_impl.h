@@ -32,6 +32,7 @@ struct marl_ctx {
     int32_t* cmap = nullptr;   // [z][y][x] cell index or -1
     float* light = nullptr;    // [z][y][x]
     float* c4 = nullptr;       // [z][y][x] species 4 after the last substep of a tick
+    bool c4_valid = false;     // c4 equals species 4 of field[cur]
     marl::CellTable t{};
     uint32_t n = 0;
     uint32_t epoch = 0;
