@@ -497,6 +497,12 @@ marl_status marl_surrogate_set_weights(marl_surrogate* s, const float* params, c
  * (y - t)^2; y_out (nullable) gets the network output [batch][16]. */
 marl_status marl_surrogate_gradients(marl_surrogate* s, const uint16_t* x, const float* t, uint32_t batch,
                                      float* grads_out, float* loss_out, float* y_out);
+/* Inference path: fused = 1 (default) runs the whole forward pass in one
+ * persistent kernel with the weights in shared memory; fused = 0 runs one
+ * GEMM launch per layer with the hidden activations in device memory.  Both
+ * compute the same function; results may differ in the last bits of the
+ * FP32 accumulation order. */
+marl_status marl_surrogate_set_inference(marl_surrogate* s, int32_t fused);
 /* Inference on device memory: x_dev standardised BF16 [n][128]; y_dev gets
  * the de-standardised deltas as [16][ldy] (species-major).  Asynchronous on
  * the surrogate's stream. */

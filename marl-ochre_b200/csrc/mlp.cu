@@ -324,6 +324,230 @@ cudaError_t launch_gemm(const GemmArgs& a, int bn, int epi, cudaStream_t s) {
     return cudaErrorInvalidValue;
 }
 
+// ------------------------------------------------------- fused inference --
+// The whole forward pass in one persistent kernel: one CTA per SM (8 warps)
+// walks 128-row tiles.  All weights stay in shared memory for the kernel's
+// life (W1 256 x 128, W2 256 x 256, W3 16 x 256: 200 KB, 128B-swizzled).  The
+// activations never leave the SM: a tile's inputs and hidden layers live in
+// tensor memory as BF16 and feed the next MMA as its A operand straight from
+// tensor memory (the TS form of tcgen05.mma; A is row-per-lane, two BF16 per
+// 32-bit column, lower k in the low half).  Tensor-memory columns: 0-255 the
+// FP32 accumulator of layers 1 and 2, 256-383 the hidden layer (BF16),
+// 384-447 the inputs (BF16), 448-463 the accumulator of layer 3.  Warp w owns
+// TMEM lanes 32(w%4).. (tile rows) and column half w/4 in the epilogues.  The
+// next tile's inputs are read from global memory into registers during
+// epilogue 1 and stored to tensor memory while layer 2 runs.
+constexpr int kFusedThreads = 256;
+constexpr uint32_t kFW1 = kHid * kInPad * 2;   // 64 KB
+constexpr uint32_t kFW2 = kHid * kHid * 2;     // 128 KB
+constexpr uint32_t kFW3 = kOut * kHid * 2;     // 8 KB
+constexpr uint32_t kFusedSmem = kFW1 + kFW2 + kFW3 + 1024;
+constexpr uint32_t kTAcc = 0, kTH = 256, kTX = 384, kTAcc3 = 448;
+
+// Copies rows [0, R) x K (K a multiple of 64) of a row-major BF16 matrix
+// into 128B-swizzled K-major atoms of R rows each.
+__device__ __forceinline__ void load_sw128(uint32_t dst, const __nv_bfloat16* src, int ld, int R, int K, int tid,
+                                           int nthreads) {
+    const int pieces = (K / 64) * R * 8;
+    for (int p = tid; p < pieces; p += nthreads) {
+        const int a = p / (R * 8), rem = p % (R * 8), r = rem >> 3, q = rem & 7;
+        cp_async16_zfill(dst + a * R * 128 + r * 128 + ((q ^ (r & 7)) << 4), src + (size_t)r * ld + a * 64 + q * 8,
+                         16u);
+    }
+}
+
+__device__ __forceinline__ void umma_bf16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Row `row` of the inputs, K half `half` (64 BF16 = 32 TMEM columns), read
+// into registers; zeros beyond M.
+__device__ __forceinline__ void load_x_half(const __nv_bfloat16* x, int M, int row, int half, uint32_t (&r)[32]) {
+    if (row < M) {
+        const uint4* src = reinterpret_cast<const uint4*>(x + (size_t)row * kInPad + half * 64);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint4 v = __ldg(src + i);
+            r[4 * i] = v.x, r[4 * i + 1] = v.y, r[4 * i + 2] = v.z, r[4 * i + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) r[i] = 0u;
+    }
+}
+
+__device__ __forceinline__ void store_x_half(uint32_t t_lane, int half, const uint32_t (&r)[32]) {
+    uint32_t lo[16], hi[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) lo[i] = r[i], hi[i] = r[16 + i];
+    tmem_st16(t_lane + kTX + half * 32, lo);
+    tmem_st16(t_lane + kTX + half * 32 + 16, hi);
+}
+
+// Epilogue of a hidden layer: columns [half*128, +128) of the accumulator ->
+// gelu(acc + bias) -> BF16 pairs into the hidden-layer columns.
+__device__ __forceinline__ void hidden_epilogue(uint32_t t_lane, int half, const float* bias) {
+#pragma unroll 1
+    for (int cb = 0; cb < 128; cb += 32) {
+        const int n = half * 128 + cb;
+        float v[16], u[16];
+        tmem_ld16(t_lane + kTAcc + n, v);
+        tmem_ld16(t_lane + kTAcc + n + 16, u);
+        uint32_t w[16];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            w[i] = pack_bf16(gelu_fast(v[2 * i] + bias[n + 2 * i]), gelu_fast(v[2 * i + 1] + bias[n + 2 * i + 1]));
+            w[8 + i] = pack_bf16(gelu_fast(u[2 * i] + bias[n + 16 + 2 * i]),
+                                 gelu_fast(u[2 * i + 1] + bias[n + 16 + 2 * i + 1]));
+        }
+        tmem_st16(t_lane + kTH + n / 2, w);
+    }
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(FusedArgs a) {
+    extern __shared__ uint8_t fsm_raw[];
+    __shared__ uint64_t bars[3];  // one per layer
+    __shared__ uint32_t tmem_slot;
+    __shared__ float sb1[kHid], sb2[kHid], sb3[kOut], sscale[kOut], sshift[kOut];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (smem_u32(fsm_raw) + 1023u) & ~1023u;
+    const uint32_t sW1 = base, sW2 = sW1 + kFW1, sW3 = sW2 + kFW2;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < 3; ++i) mbar_init(&bars[i], 1);
+        fence_mbar_init();
+    }
+    load_sw128(sW1, a.w1, kInPad, kHid, kInPad, tid, kFusedThreads);
+    load_sw128(sW2, a.w2, kHid, kHid, kHid, tid, kFusedThreads);
+    load_sw128(sW3, a.w3, kHid, kOut, kHid, tid, kFusedThreads);
+    for (int i = tid; i < kHid; i += kFusedThreads) sb1[i] = a.b1[i], sb2[i] = a.b2[i];
+    if (tid < kOut) sb3[tid] = a.b3[tid], sscale[tid] = a.scale[tid], sshift[tid] = a.shift[tid];
+    cp_async_commit_wait_all();
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const int quarter = warp & 3, half = warp >> 2;
+    const uint32_t t_lane = tmem + ((uint32_t)(quarter * 32) << 16);
+    const int ntiles = (a.M + kBM - 1) / kBM;
+    bool ok = true;
+    uint32_t it = 0;
+    uint32_t xr[32];
+    int tile = blockIdx.x;
+    if (tile < ntiles) {
+        load_x_half(a.x, a.M, tile * kBM + quarter * 32 + lane, half, xr);
+        store_x_half(t_lane, half, xr);
+        tmem_st_wait();
+    }
+    tc_fence_before();
+    __syncthreads();
+
+    for (; tile < ntiles; tile += gridDim.x, ++it) {
+        const int m0 = tile * kBM;
+        // layer 1: acc = X W1^T (A = inputs in tensor memory)
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < kInPad / 16; ++k)
+                umma_bf16_ts(tmem + kTAcc, tmem + kTX + k * 8,
+                             sw128_desc(sW1 + (k >> 2) * kHid * 128 + (k & 3) * 32), idesc_bf16(kBM, kHid),
+                             k > 0 ? 1u : 0u);
+            umma_commit(&bars[0]);
+        }
+        ok = wait_commit(&bars[0], it & 1, a.err) && ok;
+        tc_fence_after();
+        const int next = tile + gridDim.x;
+        if (next < ntiles) load_x_half(a.x, a.M, next * kBM + quarter * 32 + lane, half, xr);  // in flight
+        hidden_epilogue(t_lane, half, sb1);
+        tmem_st_wait();
+        tc_fence_before();
+        __syncthreads();
+        // layer 2: acc = H W2^T (A = hidden layer in tensor memory)
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < kHid / 16; ++k)
+                umma_bf16_ts(tmem + kTAcc, tmem + kTH + k * 8,
+                             sw128_desc(sW2 + (k >> 2) * kHid * 128 + (k & 3) * 32), idesc_bf16(kBM, kHid),
+                             k > 0 ? 1u : 0u);
+            umma_commit(&bars[1]);
+        }
+        // the next tile's inputs go to tensor memory while layer 2 runs (layer 1 is done with them)
+        if (next < ntiles) store_x_half(t_lane, half, xr);
+        ok = wait_commit(&bars[1], it & 1, a.err) && ok;
+        tc_fence_after();
+        hidden_epilogue(t_lane, half, sb2);
+        tmem_st_wait();
+        tc_fence_before();
+        __syncthreads();
+        // layer 3: acc3 = H W3^T
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < kHid / 16; ++k)
+                umma_bf16_ts(tmem + kTAcc3, tmem + kTH + k * 8,
+                             sw128_desc(sW3 + (k >> 2) * kOut * 128 + (k & 3) * 32), idesc_bf16(kBM, kOut),
+                             k > 0 ? 1u : 0u);
+            umma_commit(&bars[2]);
+        }
+        ok = wait_commit(&bars[2], it & 1, a.err) && ok;
+        tc_fence_after();
+        if (half == 0) {
+            float v[16];
+            tmem_ld16(t_lane + kTAcc3, v);
+            const int row = m0 + quarter * 32 + lane;
+            if (row < a.M && ok) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    a.y[(size_t)i * a.ldy + row] = (v[i] + sb3[i]) * sscale[i] + sshift[i];
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    tc_fence_after();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+}
+
+cudaError_t launch_mlp_fused(const FusedArgs& a, int num_sms, cudaStream_t s) {
+    if (a.M <= 0) return cudaSuccess;
+    static int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem);
+        if (e != cudaSuccess) return e;
+        configured = dev;
+    }
+    const int ntiles = (a.M + kBM - 1) / kBM;
+    k_mlp_fused<<<ntiles < num_sms ? ntiles : num_sms, kFusedThreads, kFusedSmem, s>>>(a);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------- loss -----
 // dY = 2 (y - t) / (B * 16) as BF16 [B][64] (columns 16..63 zero) and its
 // transpose [16][B]; bias gradient of the output layer and the loss sum.

@@ -60,6 +60,21 @@ struct GemmArgs {
     uint32_t* err = nullptr;           // kErr* bits on a wait timeout
 };
 
+// Arguments of the fused inference kernel: standardised BF16 inputs x
+// [M][128], BF16 weights, FP32 biases, de-standardisation, and the output
+// y [16][ldy] (species-major).
+struct FusedArgs {
+    const __nv_bfloat16* x = nullptr;
+    int M = 0;
+    const __nv_bfloat16 *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
+    const float *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
+    const float *scale = nullptr, *shift = nullptr;
+    float* y = nullptr;
+    uint32_t ldy = 0;
+    uint32_t* err = nullptr;
+};
+cudaError_t launch_mlp_fused(const FusedArgs& a, int num_sms, cudaStream_t s);
+
 // bn: 16, 128 or 256 (the instantiated tile widths for each epilogue).
 cudaError_t launch_gemm(const GemmArgs& a, int bn, int epi, cudaStream_t s);
 cudaError_t launch_loss(const float* y, const float* t, uint32_t B, __nv_bfloat16* dy, __nv_bfloat16* dyt,

@@ -191,6 +191,15 @@ marl_status surrogate_infer(marl_surrogate* s, const __nv_bfloat16* x, uint32_t 
                             cudaStream_t stream) {
     if (!s->prepared) return fail(MARL_ERR_STATE, "surrogate not prepared (marl_surrogate_prepare)");
     if (n == 0) return MARL_OK;
+    if (s->fused) {
+        mlp::FusedArgs f;
+        f.x = x, f.M = (int)n, f.w1 = s->w1, f.w2 = s->w2, f.w3 = s->w3;
+        f.b1 = s->p + mlp::kOffB1, f.b2 = s->p + mlp::kOffB2, f.b3 = s->p + mlp::kOffB3;
+        f.scale = s->norm + 2 * mlp::kIn + mlp::kOut, f.shift = s->norm + 2 * mlp::kIn;
+        f.y = y, f.ldy = ldy, f.err = s->d_err;
+        SCK(mlp::launch_mlp_fused(f, s->num_sms, stream));
+        return MARL_OK;
+    }
     SST(ensure_infer(s, n));
     mlp::GemmArgs a;
     a.err = s->d_err;
@@ -248,6 +257,7 @@ marl_status marl_surrogate_create(const marl_surrogate_config* cfg, marl_surroga
     if (st) return st;
     marl_surrogate* s = new marl_surrogate();
     s->device = dev;
+    s->num_sms = sms;
     s->cfg = *cfg;
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     s->own_stream = e == cudaSuccess;
@@ -380,6 +390,12 @@ marl_status marl_surrogate_train(marl_surrogate* s, uint32_t steps, float* loss_
     SST(check_err(s));
     if (loss_out)
         for (uint32_t i = 0; i < steps; ++i) loss_out[i] /= (float)B * mlp::kOut;
+    return MARL_OK;
+}
+
+marl_status marl_surrogate_set_inference(marl_surrogate* s, int32_t fused) {
+    if (!s) return fail(MARL_ERR_INVALID_INPUT, "null surrogate");
+    s->fused = fused != 0;
     return MARL_OK;
 }
 

@@ -10,6 +10,8 @@
 
 struct marl_surrogate {
     int device = 0;
+    int num_sms = 0;
+    bool fused = true;  // inference through the fused persistent kernel (else three GEMM launches)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     marl_surrogate_config cfg{};

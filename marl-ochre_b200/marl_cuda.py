@@ -179,7 +179,7 @@ EXPORTED = [
     "marl_surrogate_prepare", "marl_surrogate_set_lr", "marl_surrogate_train", "marl_surrogate_evaluate",
     "marl_surrogate_get_weights", "marl_surrogate_set_weights", "marl_surrogate_gradients",
     "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
-    "marl_batch_set_surrogate", "marl_batch_surrogate_counters",
+    "marl_batch_set_surrogate", "marl_batch_surrogate_counters", "marl_surrogate_set_inference",
 ]
 
 _lib = None
@@ -273,6 +273,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
         "marl_batch_set_surrogate": (c_int32, [P, P, c_int32, c_float]),
         "marl_batch_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
+        "marl_surrogate_set_inference": (c_int32, [P, c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -790,6 +791,9 @@ class Surrogate:
         _check(self.lib.marl_surrogate_gradients(self.h, _ptr(x), _ptr(tt), B, _ptr(g), ctypes.byref(loss), _ptr(y)),
                "marl_surrogate_gradients")
         return g, loss.value, y
+
+    def set_inference(self, fused: bool) -> None:
+        _check(self.lib.marl_surrogate_set_inference(self.h, 1 if fused else 0), "marl_surrogate_set_inference")
 
     def infer_device(self, x_ptr: int, n: int, y_ptr: int, ldy: int) -> None:
         _check(self.lib.marl_surrogate_infer_device(self.h, c_void_p(x_ptr), n, c_void_p(y_ptr), ldy),

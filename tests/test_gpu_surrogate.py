@@ -237,3 +237,38 @@ def test_training_gain_over_the_method_without_it(marl):
     assert after["accepted"] > zero_accept
     assert after["accepted"] > before["accepted"]
     s.close()
+
+
+@pytest.mark.parametrize("rows", [1, 127, 128, 1000, 40_000])
+def test_fused_inference_matches_layerwise_and_oracle(marl, rows):
+    """The persistent fused inference kernel against the one-GEMM-per-layer
+    path (same hardware tanh) and against the CPU restatement (exact tanh):
+    normwise relative error <= 1e-4 and <= 1e-2 (BF16 activations)."""
+    import torch
+
+    rng = np.random.default_rng(rows)
+    s = marl.Surrogate(max_pairs=128, batch=128)
+    params = random_params(rng)
+    norm = identity_norm()
+    norm[186:202] = rng.normal(0, 0.1, 16)          # output mean
+    norm[202:218] = rng.uniform(0.5, 2.0, 16)        # output std
+    s.set_weights(params, norm)
+    x = rng.normal(0, 1, (rows, 128)).astype(np.float32)
+    x[:, 93:] = 0
+    bits = mlp_ref.bf16_bits(x)
+    X = torch.from_numpy(bits.view(np.int16)).cuda()
+    y_fused = torch.full((16, rows), float("nan"), device="cuda")
+    y_layer = torch.full((16, rows), float("nan"), device="cuda")
+    s.set_inference(True)
+    s.infer_device(X.data_ptr(), rows, y_fused.data_ptr(), rows)
+    s.set_inference(False)
+    s.infer_device(X.data_ptr(), rows, y_layer.data_ptr(), rows)
+    torch.cuda.synchronize()
+    yf, yl = y_fused.cpu().numpy().T, y_layer.cpu().numpy().T
+    assert np.all(np.isfinite(yf))
+    ref = mlp_ref.forward(params, bits)[0].astype(np.float64) * norm[202:218] + norm[186:202]
+    e_layer, e_ref = normwise(yf, yl), normwise(yf, ref)
+    print(f"\nrows {rows}: fused vs layerwise {e_layer:.2e}, fused vs oracle {e_ref:.2e}")
+    assert e_layer <= 1e-4
+    assert e_ref <= 1e-2
+    s.close()
