@@ -333,11 +333,15 @@ marl_status plan_tiles(marl_batch* b, int tile, int zc, cudaStream_t s) {
         CK(cudaMalloc((void**)&b->d_diff_items, items.size() * sizeof(int4)));
         b->diff_items_cap = (int)items.size();
     }
-    // Synchronous copies: the previous contents may still be read by work
-    // already queued on `s`, so wait for it first.
+    // The copies are ordered on `s`, behind any work still reading the old
+    // maps and ahead of every launch that reads the new ones.  A plain
+    // cudaMemcpy would not do: it runs on the legacy default stream, which a
+    // non-blocking `s` does not wait for, and from pageable memory it may
+    // return before the data has landed.  The stream is synchronized before
+    // the host vectors go out of scope.
+    CK(cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b->d_diff_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
-    CK(cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->d_diff_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
     b->n_diff_items = (int)items.size();
     b->tile = tile;
     b->zc = zc;
@@ -713,6 +717,9 @@ marl_status marl_batch_create(const marl_run_spec* specs, uint32_t n_runs, const
         b->h2d += cells[r].size() * sizeof(marl_cell);
     }
     if ((st = plan_tiles(b, 0, 16, b->stream))) return bail(st);
+    // Everything issued on the legacy default stream above (copies, memsets)
+    // completes before any launch on the batch's non-blocking stream.
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(e, "marl_batch_create sync"));
     const unsigned hw = std::thread::hardware_concurrency();
     b->pool.resize((int)std::min<unsigned>(std::min<unsigned>(hw ? hw : 1, 64), n_runs) - 1);
     *out = b;
@@ -826,7 +833,7 @@ marl_status marl_batch_set_surrogate(marl_batch* b, marl_surrogate* s, int32_t m
         CK(cudaMalloc((void**)&b->surr_status, rows));
         CK(cudaMalloc((void**)&b->surr_err, rows * 4));
         CK(cudaMalloc((void**)&b->surr_counters, 64));
-        CK(cudaMemset(b->surr_counters, 0, 64));
+        CK(cudaMemsetAsync(b->surr_counters, 0, 64, b->stream));
     }
     b->surr = mode == MARL_SURR_OFF ? nullptr : s;
     b->surr_mode = mode;

@@ -317,9 +317,10 @@ marl_status marl_surrogate_upload_pairs(marl_surrogate* s, const float* rows, ui
     if (!s || (!rows && n)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     if ((uint64_t)s->rows + n > s->cfg.max_pairs)
         return fail(MARL_ERR_CAPACITY, "pair store holds %u rows", s->cfg.max_pairs);
+    // Ordered on the surrogate's stream (the kernels that read the rows run there).
+    SCK(cudaMemcpyAsync(s->raw + (size_t)s->rows * MARL_SURR_RAW_STRIDE, rows, (size_t)n * MARL_SURR_RAW_STRIDE * 4,
+                        cudaMemcpyHostToDevice, s->stream));
     SCK(cudaStreamSynchronize(s->stream));
-    SCK(cudaMemcpy(s->raw + (size_t)s->rows * MARL_SURR_RAW_STRIDE, rows, (size_t)n * MARL_SURR_RAW_STRIDE * 4,
-                   cudaMemcpyHostToDevice));
     s->rows += n;
     return MARL_OK;
 }
@@ -458,13 +459,14 @@ marl_status marl_surrogate_get_weights(marl_surrogate* s, float* params, float* 
 marl_status marl_surrogate_set_weights(marl_surrogate* s, const float* params, const float* norm) {
     if (!s) return fail(MARL_ERR_INVALID_INPUT, "null surrogate");
     SCK(cudaStreamSynchronize(s->stream));
+    // Ordered on the surrogate's stream, ahead of the kernels that read them.
     if (params) {
-        SCK(cudaMemcpy(s->p, params, (size_t)mlp::kParams * 4, cudaMemcpyHostToDevice));
+        SCK(cudaMemcpyAsync(s->p, params, (size_t)mlp::kParams * 4, cudaMemcpyHostToDevice, s->stream));
         SCK(mlp::launch_weights_bf16(s->p, s->w1, s->w2, s->w3, s->w2t, s->w3t, s->stream));
     }
     if (norm) {
         std::memcpy(s->h_norm, norm, sizeof(s->h_norm));
-        SCK(cudaMemcpy(s->norm, s->h_norm, sizeof(s->h_norm), cudaMemcpyHostToDevice));
+        SCK(cudaMemcpyAsync(s->norm, s->h_norm, sizeof(s->h_norm), cudaMemcpyHostToDevice, s->stream));
         s->prepared = true;  // explicit statistics make inference possible
     }
     SCK(cudaStreamSynchronize(s->stream));
@@ -518,7 +520,7 @@ marl_status marl_ctx_set_surrogate(marl_ctx* c, marl_surrogate* s, int32_t mode,
         SCK(cudaMalloc((void**)&c->surr_status, cap));
         SCK(cudaMalloc((void**)&c->surr_err, cap * 4));
         SCK(cudaMalloc((void**)&c->surr_counters, 64));
-        SCK(cudaMemset(c->surr_counters, 0, 64));
+        SCK(cudaMemsetAsync(c->surr_counters, 0, 64, c->stream));
     }
     c->surr = mode == MARL_SURR_OFF ? nullptr : s;
     c->surr_mode = mode;

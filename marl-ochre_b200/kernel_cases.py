@@ -70,6 +70,7 @@ def mlp_case(rows: int, reps: int, rng: np.random.Generator) -> int:
     import torch
 
     s = marl.Surrogate(max_pairs=128, batch=128)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)  # inputs are torch tensors
     params = np.zeros(marl.SURR_PARAMS, np.float32)
     params[: 256 * 128] = rng.normal(0, 0.1, 256 * 128)
     params[256 * 128 + 256: 256 * 128 + 256 + 65536] = rng.normal(0, 0.06, 65536)

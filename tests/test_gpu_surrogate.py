@@ -221,7 +221,14 @@ def test_training_gain_over_the_method_without_it(marl):
     loss = s.train(1500)
     s.set_lr(5e-4)
     loss = np.concatenate([loss, s.train(1500)])
-    after = s.evaluate(*held, tol=1e-3)
+    after = s.evaluate(*held, tol=1e-3, per_row=True)
+    s.set_inference(False)
+    layer = s.evaluate(*held, tol=1e-3, per_row=True)
+    s.set_inference(True)
+    print(f"\nfused: accepted {after['accepted']} mean err {after['mean_err']:.3e}; "
+          f"layerwise: accepted {layer['accepted']} mean err {layer['mean_err']:.3e}; "
+          f"max row diff {np.abs(after['row_err'] - layer['row_err']).max():.3e}")
+    np.testing.assert_array_equal(after["row_err"], layer["row_err"])
     raw = s.download_pairs(n_train, n - n_train)
     xt, d = raw[:, :16], raw[:, 93:109]
     plain = xt + d
@@ -248,6 +255,8 @@ def test_fused_inference_matches_layerwise_and_oracle(marl, rows):
 
     rng = np.random.default_rng(rows)
     s = marl.Surrogate(max_pairs=128, batch=128)
+    # inputs and outputs are torch tensors: order the inference on torch's stream
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
     params = random_params(rng)
     norm = identity_norm()
     norm[186:202] = rng.normal(0, 0.1, 16)          # output mean
