@@ -322,6 +322,26 @@ marl_status marl_diffuse_device_noalloc(float* field_dev, const uint8_t* occupan
                                         int32_t gz, const marl_sim_params* sim, uint32_t substeps,
                                         void* cuda_stream);
 
+/* ---- statistics ----------------------------------------------------------
+ * print_stats / print_z_profile (crates/marl-sim/src/stats.rs:9-103) reduced
+ * on the device.  Counts and the centre-column samples are exact; the three
+ * averages are FP64 (the reference sums in f32, sequentially). */
+typedef struct marl_stats {
+    uint64_t population;
+    uint64_t top, middle, bottom;   /* cells with z < Z/3, < 2(Z/3), the rest */
+    double avg_energy;              /* mean internal[0] */
+    double avg_enzyme;              /* mean internal[5] */
+    double avg_active_reactions;    /* mean count of reactions with |v_max| > 1e-9 */
+    float oxidant_top;              /* field at (X/2, Y/2, 0), species 1 */
+    float oxidant_middle;           /* (X/2, Y/2, Z/2), species 1 */
+    float reductant_bottom;         /* (X/2, Y/2, Z-1), species 2 */
+    float organic_middle;           /* (X/2, Y/2, Z/2), species 4 */
+} marl_stats;
+/* cells_per_z (nullable) gets Z counts; centre_column (nullable) gets the
+ * column (X/2, Y/2) as [5][Z]: light, then species 1 to 4 (print_z_profile's
+ * light, oxidant, reductant, carbon, organic).  Z <= 1024. */
+marl_status marl_ctx_stats(marl_ctx* ctx, marl_stats* out, uint32_t* cells_per_z, float* centre_column);
+
 /* ---- formats ------------------------------------------------------------ */
 /* Canonical 536-byte ruleset payload (crates/marl-format/src/lib.rs:70-89). */
 marl_status marl_ruleset_pack_canonical(const marl_ruleset* rs, uint8_t out[536]);

@@ -147,6 +147,13 @@ class SurrogateCounters(ctypes.Structure):
                 ("max_err", c_float)]
 
 
+class Stats(ctypes.Structure):
+    _fields_ = [("population", c_uint64), ("top", c_uint64), ("middle", c_uint64), ("bottom", c_uint64),
+                ("avg_energy", ctypes.c_double), ("avg_enzyme", ctypes.c_double),
+                ("avg_active_reactions", ctypes.c_double), ("oxidant_top", c_float), ("oxidant_middle", c_float),
+                ("reductant_bottom", c_float), ("organic_middle", c_float)]
+
+
 SURR_FEATURES = 93
 SURR_RAW_STRIDE = 112
 SURR_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 16 * 256 + 16
@@ -180,6 +187,7 @@ EXPORTED = [
     "marl_surrogate_get_weights", "marl_surrogate_set_weights", "marl_surrogate_gradients",
     "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
     "marl_batch_set_surrogate", "marl_batch_surrogate_counters", "marl_surrogate_set_inference",
+    "marl_ctx_stats",
 ]
 
 _lib = None
@@ -274,6 +282,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_batch_set_surrogate": (c_int32, [P, P, c_int32, c_float]),
         "marl_batch_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
         "marl_surrogate_set_inference": (c_int32, [P, c_int32]),
+        "marl_ctx_stats": (c_int32, [P, POINTER(Stats), P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -465,6 +474,16 @@ class Context:
         _check(self.lib.marl_mass_f64(self.h, _ptr(out)), "marl_mass_f64")
         return out
 
+    def stats(self):
+        """print_stats / print_z_profile quantities (marl_ctx_stats): (dict,
+        cells per z, centre column [5][Z] = light, species 1-4)."""
+        st = Stats()
+        Z = self.dims[2]
+        per_z = np.zeros(Z, np.uint32)
+        col = np.zeros((5, Z), np.float32)
+        _check(self.lib.marl_ctx_stats(self.h, ctypes.byref(st), _ptr(per_z), _ptr(col)), "marl_ctx_stats")
+        return {name: getattr(st, name) for name, _ in Stats._fields_}, per_z, col
+
     def diffuse_tick_with_cells(self, field: np.ndarray, occupancy: np.ndarray) -> None:
         """GpuFieldDiffuser::diffuse_tick_with_cells: `field` is updated in place."""
         X, Y, Z = self.dims
@@ -566,6 +585,16 @@ class Engine:
 
     def step(self, ticks: int = 1) -> None:
         _check(self.lib.marl_engine_step(self.h, ticks), "marl_engine_step")
+
+    def device_stats(self):
+        """marl_ctx_stats on the engine's context: (dict, cells per z, centre column [5][Z])."""
+        st = Stats()
+        Z = self.dims[2]
+        per_z = np.zeros(Z, np.uint32)
+        col = np.zeros((5, Z), np.float32)
+        _check(self.lib.marl_ctx_stats(self.lib.marl_engine_ctx(self.h), ctypes.byref(st), _ptr(per_z), _ptr(col)),
+               "marl_ctx_stats")
+        return {name: getattr(st, name) for name, _ in Stats._fields_}, per_z, col
 
     def stats(self) -> dict:
         s = EngineStats()
