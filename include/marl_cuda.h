@@ -342,6 +342,22 @@ typedef struct marl_stats {
  * light, oxidant, reductant, carbon, organic).  Z <= 1024. */
 marl_status marl_ctx_stats(marl_ctx* ctx, marl_stats* out, uint32_t* cells_per_z, float* centre_column);
 
+/* ---- binary snapshots ----------------------------------------------------
+ * The reference's field and cell dumps (crates/marl-output/src/binary_dump.rs:
+ * 109-120) and run_meta.json (crates/marl-format/src/lib.rs:130-218),
+ * uncompressed.  marl_ctx_viewer_cells packs one 25-byte ViewerCellRecord
+ * per cell on the device (marl-format lib.rs:351-364: pos 3 x f32,
+ * lineage_id u64, starter_type u8, energy f32, little endian, in
+ * cell-vector order) and copies n * 25 bytes to `out`; MARL_ERR_CAPACITY when
+ * cap_bytes is too small (*n_out still gets the count). */
+marl_status marl_ctx_viewer_cells(marl_ctx* ctx, uint8_t* out, uint64_t cap_bytes, uint32_t* n_out);
+/* Host-side writer: <dir>/run_meta.json, <dir>/tick_<tick>.field.bin (field:
+ * [z][y][x][12] f32, nullable) and <dir>/tick_<tick>.cells.bin
+ * (viewer_cells: n_cells packed records, nullable).  Each file is written to
+ * a temporary name and renamed, as the reference does. */
+marl_status marl_write_dump(const char* dir, uint64_t tick, int32_t gx, int32_t gy, int32_t gz, const float* field,
+                            const uint8_t* viewer_cells, uint32_t n_cells);
+
 /* ---- formats ------------------------------------------------------------ */
 /* Canonical 536-byte ruleset payload (crates/marl-format/src/lib.rs:70-89). */
 marl_status marl_ruleset_pack_canonical(const marl_ruleset* rs, uint8_t out[536]);

@@ -154,6 +154,32 @@ class Stats(ctypes.Structure):
                 ("reductant_bottom", c_float), ("organic_middle", c_float)]
 
 
+VIEWER_CELL_DTYPE = np.dtype([("pos", "<f4", (3,)), ("lineage_id", "<u8"), ("starter_type", "u1"),
+                              ("energy", "<f4")])  # packed, 25 bytes
+assert VIEWER_CELL_DTYPE.itemsize == 25
+
+
+def viewer_cells(ctx_handle, n: int) -> np.ndarray:
+    """marl_ctx_viewer_cells: the packed 25-byte viewer records of a context's cells."""
+    lib = load()
+    out = np.zeros(max(n, 1), VIEWER_CELL_DTYPE)
+    got = c_uint32()
+    _check(lib.marl_ctx_viewer_cells(ctx_handle, _ptr(out), out.nbytes, ctypes.byref(got)), "marl_ctx_viewer_cells")
+    return out[: got.value]
+
+
+def write_dump(directory: str, tick: int, dims, field: np.ndarray | None, cells: np.ndarray | None) -> None:
+    """marl_write_dump: run_meta.json and tick_<tick>.{field,cells}.bin under `directory`."""
+    lib = load()
+    X, Y, Z = dims
+    f = None if field is None else _as_field(np.ascontiguousarray(field, np.float32), dims)
+    c = None if cells is None else np.ascontiguousarray(cells, VIEWER_CELL_DTYPE)
+    _check(lib.marl_write_dump(os.fsencode(directory), tick, X, Y, Z, _ptr(f) if f is not None else None,
+                               _ptr(c) if c is not None and c.size else (None if c is None else
+                                                                          _ptr(np.zeros(1, np.uint8))),
+                               0 if c is None else c.size), "marl_write_dump")
+
+
 SURR_FEATURES = 93
 SURR_RAW_STRIDE = 112
 SURR_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 16 * 256 + 16
@@ -187,7 +213,7 @@ EXPORTED = [
     "marl_surrogate_get_weights", "marl_surrogate_set_weights", "marl_surrogate_gradients",
     "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
     "marl_batch_set_surrogate", "marl_batch_surrogate_counters", "marl_surrogate_set_inference",
-    "marl_ctx_stats",
+    "marl_ctx_stats", "marl_ctx_viewer_cells", "marl_write_dump",
 ]
 
 _lib = None
@@ -283,6 +309,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_batch_surrogate_counters": (c_int32, [P, POINTER(SurrogateCounters)]),
         "marl_surrogate_set_inference": (c_int32, [P, c_int32]),
         "marl_ctx_stats": (c_int32, [P, POINTER(Stats), P, P]),
+        "marl_ctx_viewer_cells": (c_int32, [P, P, c_uint64, POINTER(c_uint32)]),
+        "marl_write_dump": (c_int32, [c_char_p, c_uint64, c_int32, c_int32, c_int32, P, P, c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
