@@ -322,6 +322,54 @@ marl_status marl_diffuse_device_noalloc(float* field_dev, const uint8_t* occupan
                                         int32_t gz, const marl_sim_params* sim, uint32_t substeps,
                                         void* cuda_stream);
 
+/* ---- device fate ---------------------------------------------------------
+ * The fate step of a tick (crates/marl-sim/src/lib.rs:219-277: division
+ * placement, halving, cloning with a lineage draw and Ruleset::mutate,
+ * swap_remove deaths, appended births) performed on the device from the
+ * events the cell loop left in the table, so that ticks need no host round
+ * trip.  No counterpart call in the reference, whose fate step is host code.
+ * Random draws: one counter-based stream per dividing cell, keyed by
+ * (seed, tick, index of the parent at the start of the step) -- xoshiro256**
+ * seeded from a splitmix64 mix of the key; normals by Marsaglia's polar
+ * method with a series logarithm, so that host and device draw the same
+ * bits.  The results therefore differ from those of the host fate step
+ * (marl_engine default mode), which draws from one sequential stream.
+ * While a context runs device fate its population lives on the device; calls
+ * that need it on the host (download, count, statistics, marl_tick,
+ * marl_apply_edits, ...) synchronise the stream and fetch it. */
+typedef struct marl_fate_stats {
+    uint64_t tick;            /* tick of the next fate step */
+    uint64_t population;
+    uint64_t total_divisions; /* divisions that found a voxel, all steps */
+    uint64_t total_deaths;
+    uint64_t tick_divisions;  /* last step */
+    uint64_t tick_deaths;
+    uint64_t tick_births;     /* daughters appended (divisions minus voxel collisions) */
+    uint64_t tick_moves;      /* swap_remove moves */
+} marl_fate_stats;
+
+/* Seed of the streams, tick of the next step and the running totals. */
+marl_status marl_ctx_fate_init(marl_ctx* ctx, uint64_t seed, uint64_t tick, uint64_t total_divisions,
+                               uint64_t total_deaths);
+/* Enqueues one fate step over the current events (asynchronous). */
+marl_status marl_ctx_fate(marl_ctx* ctx);
+/* Synchronises; counters of the device fate state. */
+marl_status marl_ctx_fate_stats(marl_ctx* ctx, marl_fate_stats* out);
+/* Replaces the per-cell events (one MARL_EVENT_* per current cell), e.g. to
+ * drive marl_ctx_fate from an external cell loop. */
+marl_status marl_ctx_set_events(marl_ctx* ctx, const uint8_t* events, uint32_t n);
+/* `ticks` whole ticks (lib.rs:160-277) with device fate, enqueued on the
+ * context's stream without synchronising; device errors surface at the next
+ * synchronising call.  The surrogate must be off. */
+marl_status marl_ctx_run_ticks(marl_ctx* ctx, uint32_t ticks);
+/* Diagnostics of the stream specification (run on the current device):
+ * `count` u64 outputs of the stream keyed by (seed, tick, parent) and `count`
+ * normals(stddev) of a fresh stream with the same key; and the stream's
+ * logarithm of x[i] in (0, 1). */
+marl_status marl_fate_stream_probe(uint64_t seed, uint64_t tick, uint32_t parent, uint32_t count, float stddev,
+                                   uint64_t* u64_out, float* normal_out);
+marl_status marl_fate_stream_ln(const double* x, uint32_t n, double* out);
+
 /* ---- statistics ----------------------------------------------------------
  * print_stats / print_z_profile (crates/marl-sim/src/stats.rs:9-103) reduced
  * on the device.  Counts and the centre-column samples are exact; the three
@@ -398,6 +446,11 @@ marl_status marl_engine_get_cells(marl_engine* e, marl_cell* out, uint32_t cap, 
 marl_status marl_engine_get_field(marl_engine* e, float* field);
 marl_status marl_engine_get_light(marl_engine* e, float* light);
 marl_ctx* marl_engine_ctx(marl_engine* e);
+/* Switches the engine's fate step between the host (default: one sequential
+ * seeded stream, the reference's draw order) and the device (per-division
+ * streams keyed by the engine's rng_seed; see marl_ctx_run_ticks).  With
+ * device fate marl_engine_step enqueues all its ticks and synchronises once. */
+marl_status marl_engine_set_device_fate(marl_engine* e, int32_t enable);
 
 /* ---- batch: many independent runs advanced together --------------------
  * No counterpart in the reference, which advances one run per process

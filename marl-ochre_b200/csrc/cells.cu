@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "mlp.h"
+#include "table_ops.cuh"
 
 namespace marl {
 
@@ -59,9 +60,12 @@ __device__ __forceinline__ void schedule_cell(const CellTable& t, const Grid g, 
     t.nb[j] = nb;
 }
 
-__global__ void k_cell_schedule(CellTable t, uint32_t n, Grid g, const int32_t* __restrict__ cmap) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) schedule_cell(t, g, cmap, j);
+// n_dev (nullable): device-resident cell count, which then replaces n.
+__global__ void k_cell_schedule(CellTable t, uint32_t n, const uint32_t* __restrict__ n_dev, Grid g,
+                                const int32_t* __restrict__ cmap) {
+    if (n_dev) n = *n_dev;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        schedule_cell(t, g, cmap, j);
 }
 
 // Run of the batch that global cell index `gi` belongs to (runs are stored in
@@ -562,7 +566,8 @@ template <int MODE>
 __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constant__ CellLaunch a) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    cell_tick_loop<MODE>(S, a.k, a.n, a.ticket, a.err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    const uint32_t total = a.n_dev ? *a.n_dev : a.n;
+    cell_tick_loop<MODE>(S, a.k, total, a.ticket, a.err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv};
         j = gi;
     });
@@ -853,8 +858,6 @@ __global__ void __launch_bounds__(256) k_pack_changes(const RunDesc* __restrict_
 // memory with 16-byte loads, then its lanes write the table's arrays in
 // parallel (lane r: reaction r and internal species r; lanes < 8: transporter
 // and effector rates; lanes < 26: cold floats; lanes 26-30: scalars).
-constexpr int kRecordU4 = (int)(sizeof(marl_cell) / 16);
-static_assert(sizeof(marl_cell) % 16 == 0, "cell records are whole 16-byte words");
 constexpr int kBirthWarps = 4;
 
 __device__ __forceinline__ void birth_warp(CellTable t, const Grid g, int32_t* cmap, uint8_t* mask, uint32_t slot,
@@ -868,50 +871,7 @@ __device__ __forceinline__ void birth_warp(CellTable t, const Grid g, int32_t* c
         if (l == 0) atomicOr(err, kErrBadIndex);
         return;
     }
-    const size_t cap = t.cap;
-    const marl_ruleset& r = c.ruleset;
-    if (l < MARL_R_MAX) {
-        const marl_reaction& q = r.reactions[l];
-        const uint32_t idx = (uint32_t)q.substrate | ((uint32_t)q.product << 8) | ((uint32_t)q.catalyst << 16) |
-                             ((uint32_t)q.cofactor << 24);
-        t.rx[l * cap + slot] = make_uint4(idx, __float_as_uint(q.k_m), __float_as_uint(q.v_max), __float_as_uint(q.k_cat));
-        t.internal[l * cap + slot] = c.internal[l];
-    }
-    if (l < MARL_S_TRANSPORTERS) {
-        t.tp_rate[l * cap + slot] = make_float2(r.transport[l].uptake_rate, r.transport[l].secrete_rate);
-        t.ef_par[l * cap + slot] = make_float2(r.effectors[l].threshold, r.effectors[l].rate);
-    }
-    if (l < kColdFloats) {
-        const float v = l < 3 * MARL_S_RECEPTORS
-                            ? (l % 3 == 0 ? r.receptors[l / 3].k_half
-                                          : (l % 3 == 1 ? r.receptors[l / 3].n_hill : r.receptors[l / 3].gain))
-                            : (l == 24 ? r.hgt_propensity : r.mutation_rate);
-        t.cold[(size_t)slot * kColdFloats + l] = v;
-    }
-    if (l == 26) {
-        t.pos[slot] = pack_pos(c.pos[0], c.pos[1], c.pos[2]);
-        t.age[slot] = c.age;
-        const size_t row = (size_t)c.pos[2] * g.Y + c.pos[1];
-        cmap[row * g.X + c.pos[0]] = (int32_t)slot;
-        mask[row * mask_pitch(g.X) + c.pos[0]] = 1;
-    }
-    if (l == 27) {
-        t.state[slot] = (uint32_t)c.prep_remaining | ((uint32_t)(c.quiescent ? 1 : 0) << 16) |
-                        ((uint32_t)c.starter_type << 24);
-        t.lineage[slot] = c.lineage_id;
-    }
-    if (l == 28 || l == 29) {
-        uint32_t w[4] = {0, 0, 0, 0};
-        for (int i = 0; i < 8; ++i) {
-            const uint32_t pair = l == 28 ? ((uint32_t)r.transport[i].ext_species | ((uint32_t)r.transport[i].int_species << 8))
-                                          : ((uint32_t)r.effectors[i].int_species | ((uint32_t)r.effectors[i].ext_species << 8));
-            w[i >> 1] |= pair << ((i & 1) * 16);
-        }
-        (l == 28 ? t.tp_idx : t.ef_idx)[slot] = make_uint4(w[0], w[1], w[2], w[3]);
-    }
-    if (l == 30)
-        t.fate[slot] = make_float4(r.fate.division_energy, r.fate.death_energy, r.fate.quiescence_energy,
-                                   r.fate.division_prep_ticks);
+    write_record_warp(t, g, cmap, mask, slot, c);
 }
 
 __global__ void __launch_bounds__(32 * kBirthWarps) k_cells_from_records(const marl_cell* __restrict__ rec,
@@ -1040,42 +1000,7 @@ __global__ void k_clear_dead_batch(const RunDesc* __restrict__ runs, const uint2
     clear_dead_one(R.t, R.g, R.cmap, R.mask, items[i].y);
 }
 
-// swap_remove result (lib.rs:258-267): slot dst receives the cell in slot src.
-// Sources are >= the post-death length and destinations below it, so the
-// copies are independent.
-// One warp per move: lane l copies a few words of slot s into slot d, all
-// loads before any store.
-__device__ __forceinline__ void move_one(const CellTable& t, const Grid g, int32_t* cmap, uint32_t d, uint32_t s,
-                                         int l) {
-    const size_t cap = t.cap;
-    uint4 rx = make_uint4(0, 0, 0, 0);
-    float in = 0.0f, cold = 0.0f;
-    float2 tp = make_float2(0, 0), ef = make_float2(0, 0);
-    if (l < MARL_R_MAX) rx = t.rx[l * cap + s], in = t.internal[l * cap + s];
-    if (l < MARL_S_TRANSPORTERS) tp = t.tp_rate[l * cap + s], ef = t.ef_par[l * cap + s];
-    if (l < kColdFloats) cold = t.cold[(size_t)s * kColdFloats + l];
-    uint32_t pos = 0, age = 0, state = 0;
-    uint64_t lineage = 0;
-    uint4 w = make_uint4(0, 0, 0, 0);
-    float4 fate = make_float4(0, 0, 0, 0);
-    if (l == 26) pos = t.pos[s], age = t.age[s];
-    if (l == 27) state = t.state[s], lineage = t.lineage[s];
-    if (l == 28) w = t.tp_idx[s];
-    if (l == 29) w = t.ef_idx[s];
-    if (l == 30) fate = t.fate[s];
-    if (l < MARL_R_MAX) t.rx[l * cap + d] = rx, t.internal[l * cap + d] = in;
-    if (l < MARL_S_TRANSPORTERS) t.tp_rate[l * cap + d] = tp, t.ef_par[l * cap + d] = ef;
-    if (l < kColdFloats) t.cold[(size_t)d * kColdFloats + l] = cold;
-    if (l == 26) {
-        t.pos[d] = pos, t.age[d] = age;
-        cmap[((size_t)pos_z(pos) * g.Y + pos_y(pos)) * g.X + pos_x(pos)] = (int32_t)d;
-    }
-    if (l == 27) t.state[d] = state, t.lineage[d] = lineage;
-    if (l == 28) t.tp_idx[d] = w;
-    if (l == 29) t.ef_idx[d] = w;
-    if (l == 30) t.fate[d] = fate;
-}
-
+// swap_remove moves (lib.rs:258-267), one warp per move (move_one, table_ops.cuh).
 __global__ void k_moves(CellTable t, const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t count,
                         Grid g, int32_t* __restrict__ cmap) {
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1105,7 +1030,8 @@ static inline unsigned blocks_for(size_t n, int threads) { return (unsigned)((n 
 
 cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    k_cell_schedule<<<blocks_for(a.n, 256), 256, 0, s>>>(a.t, a.n, a.g, a.cmap);
+    const unsigned blocks = blocks_for(a.n, 256);
+    k_cell_schedule<<<blocks < 4096u ? blocks : 4096u, 256, 0, s>>>(a.t, a.n, a.n_dev, a.g, a.cmap);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@ constexpr uint32_t kFlagSpinLimit = 1u << 22;  // polls of a dependency flag (wi
 constexpr uint32_t kErrTimeoutMbar = 1u << 0;
 constexpr uint32_t kErrTimeoutDeps = 1u << 1;
 constexpr uint32_t kErrBadIndex = 1u << 2;
+constexpr uint32_t kErrCapacity = 1u << 3;   // births dropped: the cell table is full
+constexpr uint32_t kErrFateChain = 1u << 4;  // swap_remove chain longer than its level count (inconsistent events)
 
 // Packed cell position: x | y << 11 | z << 22 (x, y < 2048, z < 1024).
 constexpr int kMaxXY = 2048;

@@ -155,6 +155,7 @@ void ctx_free(marl_ctx* c) {
     for (void* p : host)
         if (p) cudaFreeHost(p);
     free_table(c->t);
+    free_fate(c->fate);
     for (auto* v : {&c->span_pool, &c->spans_pending})
         for (auto& s : *v) {
             cudaEventDestroy(s.a);
@@ -198,6 +199,10 @@ CellLaunch cell_launch(marl_ctx* c) {
     CellLaunch a;
     a.t = c->t;
     a.n = c->n;
+    if (c->n_on_device) {  // device fate: the kernels read the population
+        a.n = c->t.cap;
+        a.n_dev = &c->fate.fs->n;
+    }
     a.g = c->g;
     a.mask = c->mask;
     a.cmap = c->cmap;
@@ -236,7 +241,7 @@ marl_status enqueue_diffuse(marl_ctx* c, uint32_t substeps, bool fuse_sources, b
 }
 
 marl_status enqueue_cell_phase(marl_ctx* c) {
-    if (c->n == 0) return MARL_OK;
+    if (c->n == 0 && !c->n_on_device) return MARL_OK;
     c->c4_valid = false;  // the scatter writes every species
     CellLaunch a = cell_launch(c);
     if (c->schedule_dirty) {
@@ -318,6 +323,10 @@ marl_status collect_device_errors(marl_ctx* c, uint32_t err_bits) {
     cudaMemsetAsync(&c->d_hdr->err, 0, 4, c->stream);
     if (err_bits & (kErrTimeoutMbar | kErrTimeoutDeps))
         return fail(MARL_ERR_TIMEOUT, "device wait gave up (error bits 0x%x)", err_bits);
+    if (err_bits & kErrCapacity)
+        return fail(MARL_ERR_CAPACITY, "cell table full: births dropped (error bits 0x%x)", err_bits);
+    if (err_bits & kErrFateChain)
+        return fail(MARL_ERR_STATE, "inconsistent death events in device fate (error bits 0x%x)", err_bits);
     return fail(MARL_ERR_INVALID_INPUT, "device rejected input (error bits 0x%x)", err_bits);
 }
 
@@ -592,6 +601,10 @@ marl_status marl_download_light(marl_ctx* c, float* l) {
 
 marl_status marl_upload_cells(marl_ctx* c, const marl_cell* cells, uint32_t n) {
     if (!c || (n && !cells)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     if (n > c->t.cap) return fail(MARL_ERR_CAPACITY, "%u cells exceed capacity %u", n, c->t.cap);
     // Positions must be in the grid and unique (cell_map is a map).
     std::vector<uint8_t> seen(c->g.V(), 0);
@@ -620,6 +633,10 @@ marl_status marl_upload_cells(marl_ctx* c, const marl_cell* cells, uint32_t n) {
 
 marl_status marl_download_cells(marl_ctx* c, marl_cell* out, uint32_t cap, uint32_t* n_out) {
     if (!c || (!out && cap)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     if (n_out) *n_out = c->n;
     const uint32_t n = c->n < cap ? c->n : cap;
     if (n == 0) return MARL_OK;
@@ -636,6 +653,10 @@ marl_status marl_download_cells(marl_ctx* c, marl_cell* out, uint32_t cap, uint3
 
 marl_status marl_cell_count(marl_ctx* c, uint32_t* n) {
     if (!c || !n) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     *n = c->n;
     return MARL_OK;
 }
@@ -671,6 +692,10 @@ marl_status marl_light_update(marl_ctx* c) {
 
 marl_status marl_cell_phase(marl_ctx* c, uint8_t* events_out) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     marl_status st = enqueue_cell_phase(c);
     if (st) return st;
     if (events_out && c->n) {
@@ -682,6 +707,10 @@ marl_status marl_cell_phase(marl_ctx* c, uint8_t* events_out) {
 
 marl_status marl_tick(marl_ctx* c, marl_change* changes, uint32_t cap, uint32_t* n_changes) {
     if (!c || !n_changes || (cap && !changes)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     *n_changes = 0;
     // crates/marl-sim/src/lib.rs:164-217: sources (fused into the first
     // substep), diffusion, light, the cell loop; then the ordered change list.
@@ -720,8 +749,35 @@ marl_status marl_tick(marl_ctx* c, marl_change* changes, uint32_t cap, uint32_t*
     return MARL_OK;
 }
 
+marl_status marl_ctx_run_ticks(marl_ctx* c, uint32_t ticks) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    if (c->surr && c->surr_mode != MARL_SURR_OFF)
+        return fail(MARL_ERR_STATE, "device fate runs with the surrogate off (mode %d attached)", c->surr_mode);
+    marl_status st = begin_device_population(c);
+    if (st) return st;
+    // crates/marl-sim/src/lib.rs:160-277 per tick, all on the stream: sources
+    // (fused into the first substep), diffusion, light, the cell loop, fate.
+    const int span = span_begin(c);
+    for (uint32_t k = 0; k < ticks; ++k) {
+        bool c4_ready = false;
+        if ((st = enqueue_diffuse(c, c->sim.diffusion_substeps, true, true, &c4_ready))) return st;
+        CK(launch_light(c4_ready ? c->c4 : nullptr, c->field[c->cur], c->mask, c->light, c->g, c->fk, c->stream));
+        ++c->launches;
+        c->schedule_dirty = true;  // the previous fate step may have moved cells
+        if ((st = enqueue_cell_phase(c))) return st;
+        if ((st = enqueue_fate(c))) return st;
+        ++c->ticks;
+    }
+    span_end(c, span);
+    return MARL_OK;
+}
+
 marl_status marl_apply_edits(marl_ctx* c, const marl_edit_list* e) {
     if (!c || !e) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     const uint32_t n = c->n;
     if (e->n_deaths > n || e->n_after_deaths != n - e->n_deaths)
         return fail(MARL_ERR_INVALID_INPUT, "n_after_deaths %u != %u cells - %u deaths", e->n_after_deaths, n,

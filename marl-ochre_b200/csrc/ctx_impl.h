@@ -61,6 +61,12 @@ struct marl_ctx {
     uint8_t* d_seam_mask = nullptr;
     marl::DiffusionPlan seam_plan{};
 
+    // Device fate (fate.cu).  While n_on_device is set the population lives in
+    // fate.fs->n and `n` above is stale; sync_population brings it back.
+    marl::FateBuffers fate{};
+    bool fate_ready = false;
+    bool n_on_device = false;
+
     // Reaction surrogate (marl_ctx_set_surrogate)
     marl_surrogate* surr = nullptr;
     int surr_mode = 0;  // MARL_SURR_*
@@ -100,4 +106,11 @@ void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck);
 // Device cell table of `cap` slots (done[] and events[] zeroed).
 cudaError_t alloc_table(CellTable& t, uint32_t cap);
 void free_table(CellTable& t);
+marl_status sync_and_check(marl_ctx* c);
+marl_status collect_device_errors(marl_ctx* c, uint32_t err_bits);
+// Device fate: allocates its buffers on first use and moves the population to
+// the device; sync_population moves it back (synchronising the stream).
+marl_status begin_device_population(marl_ctx* c);
+marl_status sync_population(marl_ctx* c);
+marl_status enqueue_fate(marl_ctx* c);
 }  // namespace marl

@@ -60,6 +60,10 @@ extern "C" {
 
 marl_status marl_ctx_viewer_cells(marl_ctx* c, uint8_t* out, uint64_t cap_bytes, uint32_t* n_out) {
     if (!c || !n_out || (cap_bytes && !out)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     *n_out = c->n;
     const uint64_t bytes = (uint64_t)c->n * kViewerStride;
     if (bytes > cap_bytes) return fail(MARL_ERR_CAPACITY, "%u cells need %llu bytes", c->n, (unsigned long long)bytes);

@@ -13,6 +13,7 @@
 
 #include "../../include/marl_cuda.h"
 #include "engine_host.h"
+#include "fate_stream.h"
 #include "host_rng.h"
 
 namespace marl {
@@ -28,12 +29,6 @@ namespace {
 
 // crates/marl-sim/src/spatial.rs:8-15
 const int kFace[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-
-float rust_clamp(float v, float lo, float hi) {
-    if (v < lo) v = lo;
-    if (v > hi) v = hi;
-    return v;
-}
 
 // ---- starter metabolisms (crates/marl-sim/src/starter_metabolisms.rs) ----
 void set_inactive(marl_ruleset& r) {  // :6-42
@@ -105,69 +100,6 @@ marl_cell starter(int kind, const uint16_t pos[3], uint64_t lineage) {
     return c;
 }
 
-// ---- Ruleset::mutate (crates/marl-cell/src/cell.rs:406-524) ----
-void perturb(float& v, float rate, float sd, HostRng& rng) {
-    if (rng.f32() < rate) {
-        v += rng.normal(sd);
-        v = std::fmax(v, 0.0f);
-    }
-}
-
-void mutate_ruleset(marl_ruleset& rs, HostRng& rng, const marl_sim_params& sim) {
-    const float rate = rs.mutation_rate;
-    const float sd = sim.mutation_stddev;
-    const float structural = rate * sim.structural_mutation_rate_mult;
-    for (auto& r : rs.receptors) {
-        perturb(r.k_half, rate, sd, rng);
-        perturb(r.n_hill, rate, sd, rng);
-        r.n_hill = rust_clamp(r.n_hill, sim.hill_exponent_clamp_low, sim.hill_exponent_clamp_high);
-        perturb(r.gain, rate, sd, rng);
-    }
-    for (auto& t : rs.transport) {
-        perturb(t.uptake_rate, rate, sd, rng);
-        perturb(t.secrete_rate, rate, sd, rng);
-        if (rng.f32() < structural) t.ext_species = (uint8_t)rng.range(0, MARL_S_EXT);
-        if (rng.f32() < structural) t.int_species = (uint8_t)rng.range(0, MARL_M_INT);
-    }
-    // Gene-duplication donors: reactions active before this mutation pass.
-    std::vector<int> donors;
-    for (int i = 0; i < MARL_R_MAX; ++i)
-        if (std::fabs(rs.reactions[i].v_max) > sim.active_reaction_threshold) donors.push_back(i);
-    for (int i = 0; i < MARL_R_MAX; ++i) {
-        marl_reaction& rx = rs.reactions[i];
-        perturb(rx.k_m, rate, sd, rng);
-        perturb(rx.v_max, rate, sd, rng);
-        perturb(rx.k_cat, rate, sd, rng);
-        uint8_t marl_reaction::*slots[3] = {&marl_reaction::substrate, &marl_reaction::product,
-                                            &marl_reaction::catalyst};
-        for (auto slot : slots) {
-            if (rng.f32() < structural) {
-                const uint32_t pick = rng.range(0, (uint32_t)std::max<size_t>(donors.size(), 1));
-                if (pick < donors.size()) {
-                    const int donor = donors[pick];
-                    if (donor != i) rx.*slot = rs.reactions[donor].*slot;
-                } else {
-                    rx.*slot = (uint8_t)rng.range(0, MARL_M_INT);
-                }
-            }
-        }
-    }
-    for (auto& e : rs.effectors) {
-        perturb(e.threshold, rate, sd, rng);
-        perturb(e.rate, rate, sd, rng);
-    }
-    perturb(rs.fate.division_energy, rate, sd, rng);
-    perturb(rs.fate.death_energy, rate, sd, rng);
-    perturb(rs.fate.quiescence_energy, rate, sd, rng);
-    perturb(rs.fate.division_prep_ticks, rate, sd, rng);
-    rs.fate.division_prep_ticks = std::fmax(rs.fate.division_prep_ticks, 1.0f);
-    perturb(rs.hgt_propensity, rate, sd, rng);
-    if (rng.f32() < sim.meta_mutation_rate) {
-        rs.mutation_rate += rng.normal(sd) * sim.meta_mutation_rate;
-        rs.mutation_rate = rust_clamp(rs.mutation_rate, sim.meta_mutation_clamp_low, sim.meta_mutation_clamp_high);
-    }
-}
-
 }  // namespace
 
 namespace marl {
@@ -190,6 +122,7 @@ marl_edit_list EditData::view() const {
 void HostRun::init(int gx, int gy, int gz, const marl_sim_params& p, uint64_t seed) {
     X = gx, Y = gy, Z = gz;
     sim = p;
+    this->seed = seed;
     rng.seed_with(seed);
     cells.clear();
     cmap.assign((size_t)gx * gy * gz, -1);
@@ -304,7 +237,7 @@ marl_status HostRun::process(const marl_change* changes, uint32_t count, EditDat
                 for (int i = 0; i < MARL_M_INT; ++i) d.internal[i] = ch.internal[i] * 0.5f;
                 d.ruleset = parent.ruleset;
                 e.halve.push_back(ch.cell);
-                mutate_ruleset(d.ruleset, rng, sim);
+                marl::fate::mutate_ruleset(d.ruleset, rng, sim);  // cell.rs:406-524
                 births.push_back(d);
                 ++tick_div;
             }
@@ -358,6 +291,8 @@ marl_status HostRun::process(const marl_change* changes, uint32_t count, EditDat
 struct marl_engine {
     marl_ctx* ctx = nullptr;
     HostRun run;
+    bool device_fate = false;  // fate on the device (marl_engine_set_device_fate)
+    uint64_t population = 0;   // device fate: population after the last step
     EditData edits;
     std::vector<marl_change> changes;
     uint64_t h2d_last = 0, d2h_last = 0;
@@ -435,6 +370,23 @@ marl_status marl_engine_set_stream(marl_engine* e, void* stream) {
 
 marl_status marl_engine_step(marl_engine* e, uint32_t ticks) {
     if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    if (e->device_fate) {
+        const uint64_t h0 = marl_internal_ctx_h2d(e->ctx), d0 = marl_internal_ctx_d2h(e->ctx);
+        marl_status st = marl_ctx_run_ticks(e->ctx, ticks);
+        if (st) return st;
+        marl_fate_stats fs;
+        if ((st = marl_ctx_fate_stats(e->ctx, &fs))) return st;
+        e->run.tick = fs.tick;
+        e->run.total_div = fs.total_divisions;
+        e->run.total_death = fs.total_deaths;
+        e->run.tick_div = fs.tick_divisions;
+        e->run.tick_death = fs.tick_deaths;
+        e->population = fs.population;
+        const uint64_t t = ticks ? ticks : 1;
+        e->h2d_last = (marl_internal_ctx_h2d(e->ctx) - h0) / t;
+        e->d2h_last = (marl_internal_ctx_d2h(e->ctx) - d0) / t;
+        return MARL_OK;
+    }
     for (uint32_t t = 0; t < ticks; ++t) {
         const uint64_t h0 = marl_internal_ctx_h2d(e->ctx), d0 = marl_internal_ctx_d2h(e->ctx);
         marl_status st = e->step_once();
@@ -448,7 +400,7 @@ marl_status marl_engine_step(marl_engine* e, uint32_t ticks) {
 marl_status marl_engine_stats_get(marl_engine* e, marl_engine_stats* s) {
     if (!e || !s) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     s->tick = e->run.tick;
-    s->population = e->run.cells.size();
+    s->population = e->device_fate ? e->population : e->run.cells.size();
     s->total_divisions = e->run.total_div;
     s->total_deaths = e->run.total_death;
     s->tick_divisions = e->run.tick_div;
@@ -474,5 +426,28 @@ marl_status marl_engine_get_light(marl_engine* e, float* light) {
 }
 
 marl_ctx* marl_engine_ctx(marl_engine* e) { return e ? e->ctx : nullptr; }
+
+marl_status marl_engine_set_device_fate(marl_engine* e, int32_t enable) {
+    if (!e) return fail(MARL_ERR_INVALID_INPUT, "null engine");
+    const bool on = enable != 0;
+    if (on == e->device_fate) return MARL_OK;
+    marl_status st;
+    if (on) {
+        if ((st = marl_ctx_fate_init(e->ctx, e->run.seed, e->run.tick, e->run.total_div, e->run.total_death)))
+            return st;
+        e->population = e->run.cells.size();
+        e->device_fate = true;
+        return MARL_OK;
+    }
+    // Back to host fate: the host takes over the device's cell vector (its
+    // sequential stream continues where it stood).
+    uint32_t n = 0;
+    if ((st = marl_download_cells(e->ctx, nullptr, 0, &n))) return st;
+    std::vector<marl_cell> cells(n);
+    if (n && (st = marl_download_cells(e->ctx, cells.data(), n, &n))) return st;
+    e->run.adopt(cells.data(), n);
+    e->device_fate = false;
+    return MARL_OK;
+}
 
 }  // extern "C"

@@ -33,6 +33,7 @@ class HostRun {
     int X = 0, Y = 0, Z = 0;
     marl_sim_params sim{};
     HostRng rng;
+    uint64_t seed = 0;            // rng_seed of the run (also keys device fate streams)
     std::vector<HostCell> cells;  // the reference's `cells: Vec<CellState>` order
     std::vector<int32_t> cmap;    // the reference's `cell_map` as a dense voxel map
     uint64_t tick = 0, total_div = 0, total_death = 0, tick_div = 0, tick_death = 0;

@@ -1,0 +1,635 @@
+// Device fate processing: the reference's per-tick fate step
+// (crates/marl-sim/src/lib.rs:219-277) on the GPU, so that a tick needs no
+// host round trip.  The step consumes the events the cell loop left in the
+// table (one per cell) and performs, in the reference's semantics:
+//   * division placement (find_empty_neighbor, crates/marl-sim/src/spatial.rs:115-154)
+//     on the cell map as it stood before the step,
+//   * halving of every placed parent's internal species (lib.rs:237-240),
+//   * the daughters: clone, lineage draw, Ruleset::mutate (lib.rs:230-245),
+//   * deaths by swap_remove from the back (lib.rs:256-267),
+//   * births appended in division order unless an earlier daughter of the same
+//     step took the voxel (lib.rs:269-277).
+// Random draws come from one counter-based stream per dividing cell
+// (fate_stream.h), so every division is placed and mutated independently.
+//
+// Kernels of one step (n = cells at its start, all counts device-resident):
+//   k_fate_count / k_fate_scatter   ordered compaction of Division and Death
+//                                   events into ascending lists (2048 cells per block)
+//   k_fate_resolve (one block)      placement + voxel claims (atomicMin of the
+//                                   division ordinal), birth slots in division
+//                                   order, halving, dead voxels cleared, the
+//                                   swap_remove permutation, new population
+//   k_fate_moves                    one warp per swap_remove move
+//   k_fate_births                   one warp per daughter: gather the parent's
+//                                   row, draw + mutate on one lane, write the slot
+//
+// swap_remove in closed form.  Removing the ascending deaths d from the back
+// leaves n1 = n - |deaths| cells.  Let D(x) be the number of deaths below x,
+// b_0 = n1, and b_{k+1} = b_k + D(b_k) - D(b_{k-1}) (D(b_{-1}) = 0) until the
+// increment is zero.  The deaths below b_0 are the holes that receive cells;
+// a death q in [b_{k-1}, b_k) is first refilled from position
+// b_k + D(q) - D(b_{k-1}).  Following that map from the i-th hole's first
+// source (n1 + i) through dead positions ends at the cell that the sequential
+// back-to-front swap_remove leaves in hole i.  Each level consumes at least one
+// death, so a chain has at most as many steps as there are levels.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+#include "ctx_impl.h"
+#include "fate_stream.h"
+#include "internal.h"
+#include "table_ops.cuh"
+
+namespace marl {
+
+constexpr int kFateThreads = 256;
+constexpr int kFatePerThread = 8;
+constexpr uint32_t kFateChunk = (uint32_t)kFateThreads * kFatePerThread;
+constexpr int kResolveThreads = 512;
+constexpr int kFateBirthWarps = 4;
+constexpr uint32_t kPlacedBit = 1u << 31;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+uint32_t fate_blocks(uint32_t cap) { return (cap + kFateChunk - 1) / kFateChunk; }
+
+// crates/marl-sim/src/spatial.rs:8-15 (FACE order)
+__constant__ int c_fate_face[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+struct FateArgs {
+    FateBuffers f;
+    CellTable t;
+    Grid g;
+    int32_t* cmap;
+    uint8_t* mask;
+    uint32_t* err;
+    marl_sim_params sim;
+};
+
+__device__ __forceinline__ size_t vox_of(uint32_t P, const Grid& g) {
+    return ((size_t)pos_z(P) * g.Y + pos_y(P)) * g.X + pos_x(P);
+}
+
+// Exclusive scan of v over the block (blockDim.x a multiple of 32); `total`
+// receives the block sum.  wb: 33 words of shared memory.  Ends with a
+// barrier, so wb may be reused at once.
+__device__ __forceinline__ uint32_t block_scan_excl(uint32_t v, uint32_t* wb, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wb[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = lane < nw ? wb[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < nw) wb[lane] = wi - w;
+        if (lane == 31) wb[32] = wi;
+    }
+    __syncthreads();
+    const uint32_t r = wb[warp] + incl - v;
+    total = wb[32];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* wb) {
+    uint32_t total;
+    block_scan_excl(v, wb, total);
+    return total;
+}
+
+// Events of cells first .. first+7 (those below n).
+__device__ __forceinline__ void load_events8(const uint8_t* __restrict__ ev, uint32_t first, uint32_t n, uint8_t e[8]) {
+    if (first + 8 <= n) {
+        const uint2 w = *reinterpret_cast<const uint2*>(ev + first);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            e[i] = (uint8_t)(w.x >> (8 * i));
+            e[4 + i] = (uint8_t)(w.y >> (8 * i));
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) e[i] = first + i < n ? ev[first + i] : (uint8_t)MARL_EVENT_NONE;
+    }
+}
+
+__device__ __forceinline__ uint32_t packed_counts(const uint8_t e[8]) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        c += (e[i] == MARL_EVENT_DIVISION ? 1u : 0u) + (e[i] == MARL_EVENT_DEATH ? (1u << 16) : 0u);
+    return c;
+}
+
+__global__ void __launch_bounds__(kFateThreads) k_fate_count(const uint8_t* __restrict__ ev,
+                                                             const FateScalars* __restrict__ fs,
+                                                             uint32_t* __restrict__ blk) {
+    __shared__ uint32_t wb[33];
+    const uint32_t n = fs->n;
+    const uint32_t first = blockIdx.x * kFateChunk + threadIdx.x * kFatePerThread;
+    uint8_t e[8];
+    load_events8(ev, first, n, e);
+    const uint32_t tot = block_sum(packed_counts(e), wb);
+    if (threadIdx.x == 0) blk[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kFateThreads) k_fate_scatter(const uint8_t* __restrict__ ev, FateScalars* fs,
+                                                               const uint32_t* __restrict__ blk,
+                                                               uint32_t* __restrict__ div_list,
+                                                               uint32_t* __restrict__ death_list) {
+    __shared__ uint32_t wb[33];
+    const uint32_t n = fs->n;
+    // Offsets of this block: Division and Death counts of the blocks before it.
+    uint32_t od = 0, ox = 0;
+    for (uint32_t b = threadIdx.x; b < blockIdx.x; b += kFateThreads) {
+        const uint32_t v = blk[b];
+        od += v & 0xFFFFu;
+        ox += v >> 16;
+    }
+    od = block_sum(od, wb);
+    ox = block_sum(ox, wb);
+    const uint32_t first = blockIdx.x * kFateChunk + threadIdx.x * kFatePerThread;
+    uint8_t e[8];
+    load_events8(ev, first, n, e);
+    uint32_t tot;
+    const uint32_t ex = block_scan_excl(packed_counts(e), wb, tot);
+    uint32_t pd = od + (ex & 0xFFFFu), px = ox + (ex >> 16);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (e[i] == MARL_EVENT_DIVISION) div_list[pd++] = first + i;
+        else if (e[i] == MARL_EVENT_DEATH) death_list[px++] = first + i;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+        const uint32_t ndeath = ox + (tot >> 16);
+        fs->ndiv = od + (tot & 0xFFFFu);
+        fs->ndeath = ndeath;
+        fs->n_old = n;
+        fs->n1 = n - ndeath;
+    }
+}
+
+// find_empty_neighbor (crates/marl-sim/src/spatial.rs:115-154): the empty
+// in-grid voxels at `division_neighbor_distance` along the six faces, else the
+// empty face neighbours; one uniform pick among them.
+__device__ __forceinline__ bool place_daughter(uint32_t P, const int32_t* __restrict__ cmap, const Grid& g,
+                                               long long dist, fate::Stream& r, uint32_t& out) {
+    const long long x = pos_x(P), y = pos_y(P), z = pos_z(P);
+    uint32_t cand[6];
+    uint32_t nc = 0;
+    for (int pass = 0; pass < 2 && nc == 0; ++pass) {
+        const long long d = pass == 0 ? dist : 1;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const long long nx = x + c_fate_face[f][0] * d, ny = y + c_fate_face[f][1] * d,
+                            nz = z + c_fate_face[f][2] * d;
+            if (nx >= 0 && nx < g.X && ny >= 0 && ny < g.Y && nz >= 0 && nz < g.Z &&
+                cmap[((size_t)nz * g.Y + ny) * g.X + nx] < 0)
+                cand[nc++] = pack_pos((uint32_t)nx, (uint32_t)ny, (uint32_t)nz);
+        }
+    }
+    if (nc == 0) return false;
+    out = cand[r.range(0, nc)];
+    return true;
+}
+
+__global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_constant__ FateArgs a) {
+    __shared__ uint32_t wb[33];
+    __shared__ uint32_t s_win, s_placed, s_run, s_levels, s_err;
+    FateScalars* fs = a.f.fs;
+    const uint32_t n = fs->n_old, n1 = fs->n1, ndiv = fs->ndiv, ndeath = fs->ndeath;
+    const unsigned long long seed = fs->seed, tick = fs->tick;
+    const CellTable& t = a.t;
+    const Grid g = a.g;
+    const uint32_t cap = t.cap;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    if (tid == 0) s_win = s_placed = s_run = s_err = 0;
+
+    // A. Placement on the cell map as it stood before the step, and claims.
+    const long long dist = (long long)a.sim.division_neighbor_distance;
+    for (uint32_t k = tid; k < ndiv; k += nthr) {
+        const uint32_t p = a.f.div_list[k];
+        fate::Stream r(fate::stream_key(seed, tick, p));
+        uint32_t target = 0;
+        const bool ok = place_daughter(t.pos[p], a.cmap, g, dist, r, target);
+        a.f.div_info[k] = make_uint2(target, r.draws | (ok ? kPlacedBit : 0u));
+        if (ok) atomicMin(&a.f.claim[vox_of(target, g)], k);
+    }
+    __syncthreads();
+
+    // B. A daughter is born when its division holds the lowest ordinal among
+    // the claims on its voxel; slots follow division order.  Every placed
+    // parent is halved, whether or not its daughter survives the collision.
+    for (uint32_t base = 0; base < ndiv; base += nthr) {
+        const uint32_t k = base + tid;
+        uint32_t flags = 0;  // won | placed << 16
+        if (k < ndiv) {
+            const uint2 info = a.f.div_info[k];
+            if (info.y & kPlacedBit) flags = (1u << 16) | (a.f.claim[vox_of(info.x, g)] == k ? 1u : 0u);
+        }
+        uint32_t tot;
+        const uint32_t ex = block_scan_excl(flags, wb, tot);
+        if (k < ndiv) {
+            uint32_t slot = kFateNoSlot;
+            if (flags & 1u) {
+                const uint64_t s = (uint64_t)n1 + s_win + (ex & 0xFFFFu);
+                slot = s < cap ? (uint32_t)s : kFateDropped;
+            }
+            a.f.div_slot[k] = slot;
+            if (flags >> 16) {
+                const uint32_t p = a.f.div_list[k];
+#pragma unroll
+                for (int sp = 0; sp < MARL_M_INT; ++sp) {
+                    float& v = t.internal[(size_t)sp * cap + p];
+                    v = v * 0.5f;
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            s_win += tot & 0xFFFFu;
+            s_placed += tot >> 16;
+        }
+        __syncthreads();
+    }
+
+    // C. Dead cells leave the cell map (lib.rs:261-262).
+    for (uint32_t i = tid; i < ndeath; i += nthr) {
+        const uint32_t P = t.pos[a.f.death_list[i]];
+        const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
+        a.cmap[row * g.X + pos_x(P)] = -1;
+        a.mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
+    }
+
+    // D. cnt[o] = deaths in [n1, n1 + o) over the tail [n1, n).
+    for (uint32_t base = 0; base < ndeath; base += nthr) {
+        const uint32_t o = base + tid;
+        const uint32_t dead = (o < ndeath && t.events[n1 + o] == MARL_EVENT_DEATH) ? 1u : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_scan_excl(dead, wb, tot);
+        if (o < ndeath) a.f.cnt[o] = s_run + ex;
+        __syncthreads();
+        if (tid == 0) s_run += tot;
+        __syncthreads();
+    }
+    const uint32_t m0 = ndeath - s_run;  // holes below n1 = cells that move
+    if (tid == 0) a.f.cnt[ndeath] = s_run;
+    __syncthreads();
+
+    // E. Level boundaries b_k and D(b_{k-1}).
+    if (tid == 0) {
+        uint32_t L = 0, b = n1, db = 0;
+        for (;;) {
+            a.f.lev_b[L] = b;
+            a.f.lev_d[L] = db;
+            ++L;
+            const uint32_t Db = m0 + a.f.cnt[b - n1];
+            const uint32_t m = Db - db;
+            if (m == 0 || L > ndeath + 1) break;
+            if (m > n - b) {  // b never passes n for events consistent with the death list
+                atomicOr(&s_err, kErrFateChain);
+                break;
+            }
+            db = Db;
+            b += m;
+        }
+        s_levels = L;
+    }
+    __syncthreads();
+
+    // F. The cell that ends in hole i, and the new slot of every tail survivor.
+    const uint32_t L = s_levels;
+    for (uint32_t i = tid; i < m0; i += nthr) {
+        const uint32_t h = a.f.death_list[i];
+        uint32_t q = n1 + i;
+        uint32_t steps = 0;
+        bool bad = false;
+        while (t.events[q] == MARL_EVENT_DEATH) {
+            // level k: lev_b[k-1] <= q < lev_b[k]
+            uint32_t lo = 0, hi = L;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.f.lev_b[mid] <= q) lo = mid + 1; else hi = mid;
+            }
+            if (++steps > L || lo == 0 || lo >= L) {
+                bad = true;
+                break;
+            }
+            const uint32_t nq = a.f.lev_b[lo] + (m0 + a.f.cnt[q - n1]) - a.f.lev_d[lo];
+            if (nq >= n || nq < n1) {
+                bad = true;
+                break;
+            }
+            q = nq;
+        }
+        if (bad) atomicOr(&s_err, kErrFateChain);
+        a.f.move_dst[i] = h;
+        a.f.move_src[i] = q;
+        a.f.newidx[q - n1] = h;
+    }
+    __syncthreads();
+
+    // G. Population and counters.
+    if (tid == 0) {
+        const uint32_t room = cap - n1;
+        const uint32_t births = s_win < room ? s_win : room;
+        uint32_t err = s_err;
+        if (births < s_win) err |= kErrCapacity;
+        if (err) atomicOr(a.err, err);
+        fs->n = n1 + births;
+        fs->placed = s_placed;
+        fs->births = births;
+        fs->moves = m0;
+        fs->levels = L;
+        fs->key_tick = tick;
+        fs->tick = tick + 1;
+        fs->total_div += s_placed;
+        fs->total_death += ndeath;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fate_moves(const __grid_constant__ FateArgs a) {
+    const uint32_t moves = a.f.fs->moves;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < moves; i += warps)
+        move_one(a.t, a.g, a.cmap, a.f.move_dst[i], a.f.move_src[i], threadIdx.x & 31);
+}
+
+__global__ void __launch_bounds__(32 * kFateBirthWarps) k_fate_births(const __grid_constant__ FateArgs a) {
+    __shared__ __align__(16) marl_cell rec[kFateBirthWarps];
+    const FateScalars* fs = a.f.fs;
+    const uint32_t ndiv = fs->ndiv, n1 = fs->n1;
+    const unsigned long long seed = fs->seed, tick = fs->key_tick;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (uint32_t k = blockIdx.x * kFateBirthWarps + w; k < ndiv; k += gridDim.x * kFateBirthWarps) {
+        const uint32_t slot = a.f.div_slot[k];
+        if (slot == kFateNoSlot) continue;
+        const uint2 info = a.f.div_info[k];
+        if (l == 0) a.f.claim[vox_of(info.x, a.g)] = 0xFFFFFFFFu;  // the winner releases its voxel's claim
+        if (slot == kFateDropped) continue;
+        const uint32_t p = a.f.div_list[k];
+        const uint32_t pn = p < n1 ? p : a.f.newidx[p - n1];
+        marl_cell& c = rec[w];
+        read_record_warp(a.t, pn, c);
+        __syncwarp();
+        if (l == 0) {
+            fate::Stream r(fate::stream_key(seed, tick, p));
+            r.skip(info.y & ~kPlacedBit);
+            c.pos[0] = (uint16_t)pos_x(info.x);
+            c.pos[1] = (uint16_t)pos_y(info.x);
+            c.pos[2] = (uint16_t)pos_z(info.x);
+            c.age = 0;
+            c.prep_remaining = 0;
+            c.lineage_id = r.u64();
+            fate::mutate_ruleset(c.ruleset, r, a.sim);
+        }
+        __syncwarp();
+        write_record_warp(a.t, a.g, a.cmap, a.mask, slot, c);
+        __syncwarp();
+    }
+}
+
+__global__ void k_set_population(FateScalars* fs, uint32_t n) { fs->n = n; }
+
+__global__ void k_fate_init(FateScalars* fs, unsigned long long seed, unsigned long long tick,
+                            unsigned long long total_div, unsigned long long total_death) {
+    fs->seed = seed;
+    fs->tick = tick;
+    fs->total_div = total_div;
+    fs->total_death = total_death;
+}
+
+// Diagnostics of the stream specification: `count` u64 outputs of one stream,
+// `count` normals of a fresh stream with the same key, and stream_ln of x[].
+__global__ void k_stream_probe(unsigned long long seed, unsigned long long tick, uint32_t parent, uint32_t count,
+                               float stddev, unsigned long long* u64_out, float* normal_out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    fate::Stream a(fate::stream_key(seed, tick, parent));
+    for (uint32_t i = 0; i < count; ++i) u64_out[i] = a.u64();
+    fate::Stream b(fate::stream_key(seed, tick, parent));
+    for (uint32_t i = 0; i < count; ++i) normal_out[i] = b.normal(stddev);
+}
+
+__global__ void k_stream_ln(const double* __restrict__ x, uint32_t n, double* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = fate::stream_ln(x[i]);
+}
+
+// ----------------------------------------------------------- host side ---
+
+cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels) {
+    f = FateBuffers{};
+    cudaError_t e;
+#define A(field, type, count)                                                               \
+    if ((e = cudaMalloc((void**)&f.field, sizeof(type) * (size_t)(count))) != cudaSuccess) \
+        return e;
+    A(fs, FateScalars, 1);
+    A(blk, uint32_t, fate_blocks(cap));
+    A(div_list, uint32_t, cap);
+    A(death_list, uint32_t, cap);
+    A(div_info, uint2, cap);
+    A(div_slot, uint32_t, cap);
+    A(cnt, uint32_t, (size_t)cap + 1);
+    A(lev_b, uint32_t, (size_t)cap + 2);
+    A(lev_d, uint32_t, (size_t)cap + 2);
+    A(move_dst, uint32_t, cap);
+    A(move_src, uint32_t, cap);
+    A(newidx, uint32_t, cap);
+    A(claim, uint32_t, voxels);
+#undef A
+    if ((e = cudaMemset(f.fs, 0, sizeof(FateScalars))) != cudaSuccess) return e;
+    return cudaMemset(f.claim, 0xFF, voxels * 4);
+}
+
+void free_fate(FateBuffers& f) {
+    void* p[] = {f.fs, f.blk, f.div_list, f.death_list, f.div_info, f.div_slot, f.cnt, f.lev_b, f.lev_d,
+                 f.move_dst, f.move_src, f.newidx, f.claim};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    f = FateBuffers{};
+}
+
+cudaError_t launch_set_population(FateScalars* fs, uint32_t n, cudaStream_t s) {
+    k_set_population<<<1, 1, 0, s>>>(fs, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fate_init(FateScalars* fs, unsigned long long seed, unsigned long long tick,
+                             unsigned long long total_div, unsigned long long total_death, cudaStream_t s) {
+    k_fate_init<<<1, 1, 0, s>>>(fs, seed, tick, total_div, total_death);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fate(const FateBuffers& f, const CellTable& t, const Grid& g, int32_t* cmap, uint8_t* mask,
+                        uint32_t* err, const marl_sim_params& sim, int num_sms, cudaStream_t s) {
+    const uint32_t G = fate_blocks(t.cap);
+    k_fate_count<<<G, kFateThreads, 0, s>>>(t.events, f.fs, f.blk);
+    k_fate_scatter<<<G, kFateThreads, 0, s>>>(t.events, f.fs, f.blk, f.div_list, f.death_list);
+    FateArgs a;
+    a.f = f;
+    a.t = t;
+    a.g = g;
+    a.cmap = cmap;
+    a.mask = mask;
+    a.err = err;
+    a.sim = sim;
+    k_fate_resolve<<<1, kResolveThreads, 0, s>>>(a);
+    k_fate_moves<<<num_sms, 256, 0, s>>>(a);
+    k_fate_births<<<2 * num_sms, 32 * kFateBirthWarps, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace marl
+
+using namespace marl;
+
+#define CK(expr)                                            \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+    } while (0)
+
+namespace marl {
+
+marl_status begin_device_population(marl_ctx* c) {
+    if (!c->fate_ready) {
+        CK(alloc_fate(c->fate, c->t.cap, c->g.V()));
+        c->fate_ready = true;
+    }
+    if (!c->n_on_device) {
+        CK(launch_set_population(c->fate.fs, c->n, c->stream));
+        c->n_on_device = true;
+        c->schedule_dirty = true;
+    }
+    return MARL_OK;
+}
+
+marl_status sync_population(marl_ctx* c) {
+    if (!c->n_on_device) return MARL_OK;
+    uint32_t n = 0;
+    CK(cudaMemcpyAsync(c->h_hdr, c->d_hdr, sizeof(ChangeHeader), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&n, &c->fate.fs->n, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->d2h_bytes += sizeof(ChangeHeader) + 4;
+    c->n = n;
+    c->n_on_device = false;
+    c->schedule_dirty = true;
+    return collect_device_errors(c, c->h_hdr->err);
+}
+
+marl_status enqueue_fate(marl_ctx* c) {
+    marl_status st = begin_device_population(c);
+    if (st) return st;
+    c->c4_valid = false;
+    CK(launch_fate(c->fate, c->t, c->g, c->cmap, c->mask, &c->d_hdr->err, c->sim, c->num_sms, c->stream));
+    c->launches += 5;
+    c->schedule_dirty = true;
+    return MARL_OK;
+}
+
+}  // namespace marl
+
+extern "C" {
+
+marl_status marl_ctx_fate_init(marl_ctx* c, uint64_t seed, uint64_t tick, uint64_t total_divisions,
+                               uint64_t total_deaths) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    marl_status st = begin_device_population(c);
+    if (st) return st;
+    CK(launch_fate_init(c->fate.fs, seed, tick, total_divisions, total_deaths, c->stream));
+    return MARL_OK;
+}
+
+marl_status marl_ctx_fate(marl_ctx* c) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    return enqueue_fate(c);
+}
+
+marl_status marl_ctx_fate_stats(marl_ctx* c, marl_fate_stats* out) {
+    if (!c || !out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    marl_status st = begin_device_population(c);
+    if (st) return st;
+    FateScalars h;
+    CK(cudaMemcpyAsync(&h, c->fate.fs, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    st = sync_and_check(c);
+    c->d2h_bytes += sizeof(h);
+    if (st) return st;
+    out->tick = h.tick;
+    out->population = h.n;
+    out->total_divisions = h.total_div;
+    out->total_deaths = h.total_death;
+    out->tick_divisions = h.placed;
+    out->tick_deaths = h.ndeath;
+    out->tick_births = h.births;
+    out->tick_moves = h.moves;
+    return MARL_OK;
+}
+
+marl_status marl_ctx_set_events(marl_ctx* c, const uint8_t* events, uint32_t n) {
+    if (!c || (n && !events)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    marl_status st = sync_population(c);
+    if (st) return st;
+    if (n != c->n) return fail(MARL_ERR_INVALID_INPUT, "%u events for %u cells", n, c->n);
+    for (uint32_t i = 0; i < n; ++i)
+        if (events[i] > MARL_EVENT_QUIESCENCE) return fail(MARL_ERR_INVALID_INPUT, "event %u of cell %u", events[i], i);
+    if (n) {
+        CK(cudaMemcpyAsync(c->t.events, events, n, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->h2d_bytes += n;
+    }
+    return MARL_OK;
+}
+
+marl_status marl_fate_stream_probe(uint64_t seed, uint64_t tick, uint32_t parent, uint32_t count, float stddev,
+                                   uint64_t* u64_out, float* normal_out) {
+    if (!u64_out || !normal_out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (count == 0) return MARL_OK;
+    int dev, sms;
+    marl_status st = check_device(&dev, &sms);
+    if (st) return st;
+    unsigned long long* du = nullptr;
+    float* dn = nullptr;
+    CK(cudaMalloc((void**)&du, (size_t)count * 8));
+    cudaError_t e = cudaMalloc((void**)&dn, (size_t)count * 4);
+    if (e == cudaSuccess) {
+        k_stream_probe<<<1, 32>>>(seed, tick, parent, count, stddev, du, dn);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(u64_out, du, (size_t)count * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(normal_out, dn, (size_t)count * 4, cudaMemcpyDeviceToHost);
+    cudaFree(du);
+    if (dn) cudaFree(dn);
+    if (e != cudaSuccess) return cuda_fail(e, "marl_fate_stream_probe");
+    return MARL_OK;
+}
+
+marl_status marl_fate_stream_ln(const double* x, uint32_t n, double* out) {
+    if (!x || !out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (n == 0) return MARL_OK;
+    int dev, sms;
+    marl_status st = check_device(&dev, &sms);
+    if (st) return st;
+    double* d = nullptr;
+    CK(cudaMalloc((void**)&d, (size_t)n * 16));
+    cudaError_t e = cudaMemcpy(d, x, (size_t)n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_stream_ln<<<(n + 255) / 256, 256>>>(d, n, d + n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + n, (size_t)n * 8, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "marl_fate_stream_ln");
+    return MARL_OK;
+}
+
+}  // extern "C"

@@ -138,7 +138,8 @@ struct CellLaunch {
     int mode = kModePlain;
     SurrView sv;
     CellTable t;
-    uint32_t n;
+    uint32_t n;                     // cells (an upper bound when n_dev is set)
+    const uint32_t* n_dev = nullptr;  // device-resident cell count (device fate), read by the kernels
     Grid g;
     const uint8_t* mask;
     const int32_t* cmap;
@@ -177,5 +178,54 @@ cudaError_t launch_moves(CellTable t, const uint32_t* dst, const uint32_t* src, 
                          int32_t* cmap, cudaStream_t s);
 cudaError_t launch_rebuild_maps(const CellTable& t, uint32_t n, const Grid& g, int32_t* cmap, uint8_t* mask,
                                 cudaStream_t s);
+
+// ---- device fate (fate.cu) ----
+// Scalars of a context's device fate processing.  While the context runs
+// device fate the population lives here (n) and the host copy is stale.
+struct FateScalars {
+    unsigned long long seed;         // run seed of the per-division streams
+    unsigned long long tick;         // tick of the next fate step
+    unsigned long long key_tick;     // tick the last step's streams were keyed by
+    unsigned long long total_div;    // divisions that found a voxel, all steps
+    unsigned long long total_death;
+    uint32_t n;       // population
+    uint32_t n_old;   // population at the start of the last step
+    uint32_t n1;      // after its deaths
+    uint32_t ndiv;    // Division events of the last step
+    uint32_t ndeath;  // Death events of the last step
+    uint32_t placed;  // divisions of the last step that found a voxel
+    uint32_t births;  // daughters appended by the last step
+    uint32_t moves;   // swap_remove moves of the last step
+    uint32_t levels;  // swap_remove levels of the last step
+    uint32_t pad[5];
+};
+
+// Scratch of device fate over a table of `cap` slots and a grid of V voxels.
+struct FateBuffers {
+    FateScalars* fs = nullptr;
+    uint32_t* blk = nullptr;         // [fate_blocks(cap)] packed Division | Death << 16 counts per chunk
+    uint32_t* div_list = nullptr;    // [cap] dividing cells, ascending
+    uint32_t* death_list = nullptr;  // [cap] dying cells, ascending
+    uint2* div_info = nullptr;       // [cap] (packed target voxel, stream draws | placed << 31)
+    uint32_t* div_slot = nullptr;    // [cap] birth slot of division k, or kFateNoSlot / kFateDropped
+    uint32_t* cnt = nullptr;         // [cap + 1] deaths in [n1, n1 + o) for tail offset o
+    uint32_t* lev_b = nullptr;       // [cap + 2] swap_remove level boundaries
+    uint32_t* lev_d = nullptr;       // [cap + 2] deaths below the previous boundary
+    uint32_t* move_dst = nullptr;    // [cap]
+    uint32_t* move_src = nullptr;    // [cap]
+    uint32_t* newidx = nullptr;      // [cap] new slot of the tail survivor at offset o
+    uint32_t* claim = nullptr;       // [V] lowest division ordinal claiming the voxel, else 0xFFFFFFFF
+};
+constexpr uint32_t kFateNoSlot = 0xFFFFFFFFu;
+constexpr uint32_t kFateDropped = 0xFFFFFFFEu;
+uint32_t fate_blocks(uint32_t cap);
+cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels);
+void free_fate(FateBuffers& f);
+cudaError_t launch_set_population(FateScalars* fs, uint32_t n, cudaStream_t s);
+cudaError_t launch_fate_init(FateScalars* fs, unsigned long long seed, unsigned long long tick,
+                             unsigned long long total_div, unsigned long long total_death, cudaStream_t s);
+// The fate step over the events of the table's first fs->n cells.
+cudaError_t launch_fate(const FateBuffers& f, const CellTable& t, const Grid& g, int32_t* cmap, uint8_t* mask,
+                        uint32_t* err, const marl_sim_params& sim, int num_sms, cudaStream_t s);
 
 }  // namespace marl

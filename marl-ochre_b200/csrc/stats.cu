@@ -85,6 +85,10 @@ extern "C" {
 marl_status marl_ctx_stats(marl_ctx* c, marl_stats* out, uint32_t* cells_per_z, float* centre_column) {
     if (!c || !out) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     if (c->g.Z > kStatsMaxZ) return fail(MARL_ERR_INVALID_INPUT, "Z %d above %d", c->g.Z, kStatsMaxZ);
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
     const Grid g = c->g;
     cudaStream_t s = c->stream;
     StatsAccum* d = nullptr;

@@ -154,6 +154,12 @@ class Stats(ctypes.Structure):
                 ("reductant_bottom", c_float), ("organic_middle", c_float)]
 
 
+class FateStats(ctypes.Structure):
+    _fields_ = [(name, c_uint64) for name in (
+        "tick", "population", "total_divisions", "total_deaths", "tick_divisions", "tick_deaths", "tick_births",
+        "tick_moves")]
+
+
 VIEWER_CELL_DTYPE = np.dtype([("pos", "<f4", (3,)), ("lineage_id", "<u8"), ("starter_type", "u1"),
                               ("energy", "<f4")])  # packed, 25 bytes
 assert VIEWER_CELL_DTYPE.itemsize == 25
@@ -214,6 +220,8 @@ EXPORTED = [
     "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
     "marl_batch_set_surrogate", "marl_batch_surrogate_counters", "marl_surrogate_set_inference",
     "marl_ctx_stats", "marl_ctx_viewer_cells", "marl_write_dump",
+    "marl_ctx_fate_init", "marl_ctx_fate", "marl_ctx_fate_stats", "marl_ctx_set_events", "marl_ctx_run_ticks",
+    "marl_fate_stream_probe", "marl_fate_stream_ln", "marl_engine_set_device_fate",
 ]
 
 _lib = None
@@ -311,6 +319,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_stats": (c_int32, [P, POINTER(Stats), P, P]),
         "marl_ctx_viewer_cells": (c_int32, [P, P, c_uint64, POINTER(c_uint32)]),
         "marl_write_dump": (c_int32, [c_char_p, c_uint64, c_int32, c_int32, c_int32, P, P, c_uint32]),
+        "marl_ctx_fate_init": (c_int32, [P, c_uint64, c_uint64, c_uint64, c_uint64]),
+        "marl_ctx_fate": (c_int32, [P]),
+        "marl_ctx_fate_stats": (c_int32, [P, POINTER(FateStats)]),
+        "marl_ctx_set_events": (c_int32, [P, P, c_uint32]),
+        "marl_ctx_run_ticks": (c_int32, [P, c_uint32]),
+        "marl_fate_stream_probe": (c_int32, [c_uint64, c_uint64, c_uint32, c_uint32, c_float, P, P]),
+        "marl_fate_stream_ln": (c_int32, [P, c_uint32, P]),
+        "marl_engine_set_device_fate": (c_int32, [P, c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -512,6 +528,27 @@ class Context:
         _check(self.lib.marl_ctx_stats(self.h, ctypes.byref(st), _ptr(per_z), _ptr(col)), "marl_ctx_stats")
         return {name: getattr(st, name) for name, _ in Stats._fields_}, per_z, col
 
+    # device fate
+    def fate_init(self, seed: int, tick: int = 0, total_divisions: int = 0, total_deaths: int = 0) -> None:
+        _check(self.lib.marl_ctx_fate_init(self.h, seed, tick, total_divisions, total_deaths), "marl_ctx_fate_init")
+
+    def fate(self) -> None:
+        """Enqueue one device fate step over the current events."""
+        _check(self.lib.marl_ctx_fate(self.h), "marl_ctx_fate")
+
+    def fate_stats(self) -> dict:
+        st = FateStats()
+        _check(self.lib.marl_ctx_fate_stats(self.h, ctypes.byref(st)), "marl_ctx_fate_stats")
+        return {name: getattr(st, name) for name, _ in FateStats._fields_}
+
+    def set_events(self, events: np.ndarray) -> None:
+        ev = np.ascontiguousarray(events, np.uint8)
+        _check(self.lib.marl_ctx_set_events(self.h, _ptr(ev) if ev.size else None, ev.size), "marl_ctx_set_events")
+
+    def run_ticks(self, ticks: int = 1) -> None:
+        """Whole ticks with device fate, enqueued without synchronising."""
+        _check(self.lib.marl_ctx_run_ticks(self.h, ticks), "marl_ctx_run_ticks")
+
     def diffuse_tick_with_cells(self, field: np.ndarray, occupancy: np.ndarray) -> None:
         """GpuFieldDiffuser::diffuse_tick_with_cells: `field` is updated in place."""
         X, Y, Z = self.dims
@@ -522,6 +559,25 @@ class Context:
         if occ.size != X * Y * Z:
             raise MarlError(1, "diffuse_tick_with_cells", f"occupancy has {occ.size} voxels, expected {X * Y * Z}")
         _check(self.lib.marl_diffuse_tick_with_cells(self.h, _ptr(field), _ptr(occ)), "marl_diffuse_tick_with_cells")
+
+
+def fate_stream_probe(seed: int, tick: int, parent: int, count: int, stddev: float = 1.0):
+    """marl_fate_stream_probe: `count` u64 draws and `count` normals of the
+    device-fate stream keyed by (seed, tick, parent), computed on the GPU."""
+    lib = load()
+    u = np.zeros(max(count, 1), np.uint64)
+    z = np.zeros(max(count, 1), np.float32)
+    _check(lib.marl_fate_stream_probe(seed, tick, parent, count, stddev, _ptr(u), _ptr(z)), "marl_fate_stream_probe")
+    return u[:count], z[:count]
+
+
+def fate_stream_ln(x: np.ndarray) -> np.ndarray:
+    """marl_fate_stream_ln: the device-fate streams' logarithm, on the GPU."""
+    lib = load()
+    xs = np.ascontiguousarray(x, np.float64)
+    out = np.zeros(max(xs.size, 1), np.float64)
+    _check(lib.marl_fate_stream_ln(_ptr(xs), xs.size, _ptr(out)), "marl_fate_stream_ln")
+    return out[:xs.size]
 
 
 def diffuse_device(field_ptr: int, scratch_ptr: int, occ_ptr: int, dims, params: SimParams, substeps: int,
@@ -613,6 +669,10 @@ class Engine:
 
     def step(self, ticks: int = 1) -> None:
         _check(self.lib.marl_engine_step(self.h, ticks), "marl_engine_step")
+
+    def set_device_fate(self, enable: bool = True) -> None:
+        """Fate on the device (per-division streams keyed by rng_seed) or on the host."""
+        _check(self.lib.marl_engine_set_device_fate(self.h, 1 if enable else 0), "marl_engine_set_device_fate")
 
     def device_stats(self):
         """marl_ctx_stats on the engine's context: (dict, cells per z, centre column [5][Z])."""

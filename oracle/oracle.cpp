@@ -406,7 +406,8 @@ static void apply_deltas_to_neighbors(const uint16_t pos[3], T* field, const int
 }
 
 // crates/marl-sim/src/spatial.rs:115-154 (find_empty_neighbor)
-static bool find_empty_neighbor(const uint16_t pos[3], const int32_t* cmap, const Dims& g, Rng& rng,
+template <class R>
+static bool find_empty_neighbor(const uint16_t pos[3], const int32_t* cmap, const Dims& g, R& rng,
                                 const marl_sim_params& sim, uint16_t out[3]) {
     const int dist = (int)sim.division_neighbor_distance;
     uint16_t cand[6][3];
@@ -448,14 +449,16 @@ static bool find_empty_neighbor(const uint16_t pos[3], const int32_t* cmap, cons
 // ------------------------------------------------------------- mutation ----
 
 // crates/marl-cell/src/cell.rs:406-524 (Ruleset::mutate) over the stand-in RNG.
-static void maybe_mutate(float& v, float rate, float stddev, Rng& rng) {
+template <class R>
+static void maybe_mutate(float& v, float rate, float stddev, R& rng) {
     if (rng.next_f32() < rate) {
         v += rng.normal(stddev);
         v = std::fmax(v, 0.0f);
     }
 }
 
-void mutate(marl_ruleset& rs, Rng& rng, const marl_sim_params& sim) {
+template <class R>
+void mutate(marl_ruleset& rs, R& rng, const marl_sim_params& sim) {
     const float rate = rs.mutation_rate;
     const float sd = sim.mutation_stddev;
     const float smr = rate * sim.structural_mutation_rate_mult;
@@ -619,13 +622,15 @@ struct World {
     Dims g;
     marl_sim_params p;
     Rng rng;
+    uint64_t seed;
+    int fate_mode = 0;  // 0: one sequential stream (rng); 1: per-division streams keyed by (seed, tick, parent)
     std::vector<float> field, light;
     std::vector<int32_t> cmap;  // HashMap<[u16;3], usize> as a dense voxel map
     std::vector<marl_cell> cells;
     uint64_t total_div = 0, total_death = 0, tick_div = 0, tick_death = 0, tick = 0;
 
     World(int X, int Y, int Z, const marl_sim_params& sp, uint64_t seed)
-        : g{X, Y, Z}, p(sp), rng(seed), field(g.V() * 12, 0.0f), light(g.V(), 0.0f), cmap(g.V(), -1) {}
+        : g{X, Y, Z}, p(sp), rng(seed), seed(seed), field(g.V() * 12, 0.0f), light(g.V(), 0.0f), cmap(g.V(), -1) {}
 
     void rebuild_map() {
         std::fill(cmap.begin(), cmap.end(), -1);
@@ -714,7 +719,23 @@ struct World {
         for (size_t i = 0; i < events.size(); ++i) {
             if (events[i] == MARL_EVENT_DIVISION) {
                 uint16_t dpos[3];
-                if (find_empty_neighbor(cells[i].pos, cmap.data(), g, rng, p, dpos)) {
+                if (fate_mode == 1) {
+                    FateRng r(seed, tick, (uint32_t)i);
+                    if (find_empty_neighbor(cells[i].pos, cmap.data(), g, r, p, dpos)) {
+                        marl_cell d = cells[i];
+                        std::memcpy(d.pos, dpos, sizeof(dpos));
+                        d.age = 0;
+                        d.prep_remaining = 0;
+                        d.lineage_id = r.next_u64();
+                        for (int k = 0; k < MARL_M_INT; ++k) {
+                            d.internal[k] *= 0.5f;
+                            cells[i].internal[k] *= 0.5f;
+                        }
+                        mutate(d.ruleset, r, p);
+                        births.push_back(d);
+                        ++tick_div;
+                    }
+                } else if (find_empty_neighbor(cells[i].pos, cmap.data(), g, rng, p, dpos)) {
                     marl_cell d = cells[i];
                     std::memcpy(d.pos, dpos, sizeof(dpos));
                     d.age = 0;
@@ -957,6 +978,20 @@ void oracle_world_fate(void* w, const int32_t* events, uint32_t n) {
 void oracle_world_tick(void* w, uint32_t ticks) {
     World* W = (World*)w;
     for (uint32_t t = 0; t < ticks; ++t) W->full_tick();
+}
+void oracle_world_set_fate_mode(void* w, int mode) { ((World*)w)->fate_mode = mode; }
+void oracle_world_set_tick(void* w, uint64_t tick) { ((World*)w)->tick = tick; }
+// Stream of device fate: `count` u64 draws, and `count` normals of a fresh
+// stream with the same key.
+void oracle_fate_stream(uint64_t seed, uint64_t tick, uint32_t parent, uint32_t count, float stddev, uint64_t* u64_out,
+                        float* normal_out) {
+    FateRng a(seed, tick, parent);
+    for (uint32_t i = 0; i < count; ++i) u64_out[i] = a.next_u64();
+    FateRng b(seed, tick, parent);
+    for (uint32_t i = 0; i < count; ++i) normal_out[i] = b.normal(stddev);
+}
+void oracle_fate_log(const double* x, uint32_t n, double* out) {
+    for (uint32_t i = 0; i < n; ++i) out[i] = fate_log(x[i]);
 }
 void oracle_world_stats(void* w, uint64_t out[6]) {
     World* W = (World*)w;

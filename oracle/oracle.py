@@ -75,6 +75,10 @@ def lib() -> ctypes.CDLL:
         "oracle_world_fate": (None, [P, P, c_uint32]),
         "oracle_world_tick": (None, [P, c_uint32]),
         "oracle_world_stats": (None, [P, P]),
+        "oracle_world_set_fate_mode": (None, [P, c_int]),
+        "oracle_world_set_tick": (None, [P, c_uint64]),
+        "oracle_fate_stream": (None, [c_uint64, c_uint64, c_uint32, c_uint32, c_float, P, P]),
+        "oracle_fate_log": (None, [P, c_uint32, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -206,6 +210,23 @@ def mutate(ruleset: np.ndarray, rng_state: np.ndarray, params: SimParams) -> np.
     return r[0]
 
 
+def fate_stream(seed: int, tick: int, parent: int, count: int, stddev: float = 1.0):
+    """Device-fate stream keyed by (seed, tick, parent): `count` u64 draws and
+    `count` normals(stddev) of a fresh stream with the same key."""
+    u = np.zeros(max(count, 1), np.uint64)
+    z = np.zeros(max(count, 1), np.float32)
+    lib().oracle_fate_stream(seed, tick, parent, count, stddev, _p(u), _p(z))
+    return u[:count], z[:count]
+
+
+def fate_log(x: np.ndarray) -> np.ndarray:
+    """The device-fate streams' logarithm of x in (0, 1)."""
+    xs = np.ascontiguousarray(x, np.float64)
+    out = np.zeros(max(xs.size, 1), np.float64)
+    lib().oracle_fate_log(_p(xs), xs.size, _p(out))
+    return out[:xs.size]
+
+
 class World:
     """Stateful restatement of marl_sim::run's state (field, light, cells, cell_map, rng)."""
 
@@ -289,6 +310,14 @@ class World:
 
     def tick(self, n: int = 1) -> None:
         lib().oracle_world_tick(self.h, n)
+
+    def set_fate_mode(self, mode: int) -> None:
+        """0: fate draws from the run's one sequential stream (host engine);
+        1: one stream per division keyed by (seed, tick, parent) (device fate)."""
+        lib().oracle_world_set_fate_mode(self.h, mode)
+
+    def set_tick(self, tick: int) -> None:
+        lib().oracle_world_set_tick(self.h, tick)
 
     def stats(self) -> dict:
         out = np.zeros(6, np.uint64)
