@@ -244,16 +244,65 @@ ENSEMBLE_GRIDS = [(64, 64, 32), (96, 96, 48), (128, 128, 64), (128, 128, 96)]
 MLP_FLOP_PER_CELL = 2 * (93 * 256 + 256 * 256 + 256 * 16)  # algorithmic forward FLOPs (93 inputs)
 
 
+def device_fate_leg(marl, torch, stream, steps: int, warmup: int, flush) -> dict:
+    """The same default run with fate on the device (per-division streams keyed
+    by the run seed): every tick through marl_engine_step with an L2 flush
+    between ticks, then `steps` more ticks enqueued by one marl_engine_step call."""
+    eng = marl.Engine(DIMS, marl.default_params(), rng_seed=SEED, seed_count=SEED_COUNT, cell_capacity=1 << 20)
+    eng.set_stream(stream.cuda_stream)
+    eng.autotune(5)
+    eng.set_device_fate(True)
+    eng.step(warmup)
+    torch.cuda.synchronize()
+    c0 = eng.counters()
+    wall = 0.0
+    h2d = d2h = 0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.step(1)
+        torch.cuda.synchronize()
+        wall += time.perf_counter() - t0
+        s = eng.stats()
+        h2d += s["h2d_bytes_last_tick"]
+        d2h += s["d2h_bytes_last_tick"]
+    c1 = eng.counters()
+    st = eng.stats()
+    dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.step(steps)
+    torch.cuda.synchronize()
+    wall_one_call = time.perf_counter() - t0
+    st2 = eng.stats()
+    eng.close()
+    return {"e2e_ticks_per_s": steps / wall, "device_ticks_per_s": steps / dev_s,
+            "one_call_ticks_per_s": steps / wall_one_call,
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "launches_per_tick": (c1["kernel_launches"] - c0["kernel_launches"]) / steps,
+            "population_end": int(st["population"]), "divisions": int(st["total_divisions"]),
+            "deaths": int(st["total_deaths"]),
+            "one_call_ticks": f"{warmup + steps + 1}..{warmup + 2 * steps}",
+            "one_call_population_end": int(st2["population"]),
+            "api": "marl_engine_step (C ABI) with marl_engine_set_device_fate: per tick, wall clock incl. the "
+                   "64-byte fate-counter read; one_call: all ticks in one call, one synchronisation",
+            "note": "fate on the device draws from per-division streams, so the run's trajectory differs from "
+                    "the host-fate run (same model, different random numbers)"}
+
+
 def ensemble_leg(marl, torch, stream, ticks: int = 30, warmup: int = 3, surrogate=None) -> dict:
     """Batched ensemble: 64 runs (seeds 0-63), 16 each of four grid sizes, one
     launch per phase for all runs, graph-captured device tick; with a trained
     surrogate, the same ticks again in the gated mode at 1e-3."""
 
-    def timed(mode):
+    def timed(mode, device_fate=False):
         runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
         b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=1 << 16)
         b.set_stream(stream.cuda_stream)
         us = b.autotune(3)
+        if device_fate:
+            b.set_device_fate(True)
         if mode is not None:
             b.set_surrogate(surrogate, mode, 1e-3)
         b.step(warmup)
@@ -282,6 +331,10 @@ def ensemble_leg(marl, torch, stream, ticks: int = 30, warmup: int = 3, surrogat
                    "copies; e2e adds the host fate step of all runs on worker threads")
     if surrogate is not None:
         res["with_surrogate_gated_1e-3"] = timed(marl.SURR_GATED)
+    res["with_device_fate"] = timed(None, device_fate=True)
+    res["with_device_fate"]["note"] = ("fate of every run on the device: one CUDA graph per batch tick, one "
+                                       "synchronisation per step call; per-division random streams, so the "
+                                       "trajectories differ from the host-fate runs")
     return res
 
 
@@ -510,6 +563,7 @@ def main() -> int:
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate leg")
     ap.add_argument("--no-micro", action="store_true", help="skip the field and cell microbenchmarks")
+    ap.add_argument("--no-device-fate", action="store_true", help="skip the device-fate engine leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -577,7 +631,9 @@ def main() -> int:
     roof = None
     if rank == 0 and not args.no_roofline:
         roof = diffusion_roofline(marl, torch, eng, stream, tuple(args.tile) if args.tile else None)
-    ens = surr = fmicro = cmicro = None
+    ens = surr = fmicro = cmicro = dfate = None
+    if rank == 0 and world == 1 and not args.no_device_fate:
+        dfate = device_fate_leg(marl, torch, stream, args.steps, args.warmup, flush)
     if rank == 0 and world == 1 and not args.no_micro:
         fmicro = field_microbench_leg(marl, torch, stream)
         cmicro = cell_microbench_leg(marl, torch, stream)
@@ -605,6 +661,7 @@ def main() -> int:
             "e2e": {"value": e2e, "unit": "ticks/s", "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
                     "api": "marl_engine_step (C ABI), wall clock per tick"},
+            "e2e_device_fate": dfate,
             "clocks": clocks,
             "gpu_launches": int(launches),
             "field_microbench": fmicro,

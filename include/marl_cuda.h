@@ -496,6 +496,11 @@ marl_status marl_batch_get_field(marl_batch* b, uint32_t run, float* field);
 marl_status marl_batch_get_light(marl_batch* b, uint32_t run, float* light);
 /* As marl_ctx_counters, over the whole batch (ticks counts batch ticks). */
 marl_status marl_batch_counters(marl_batch* b, marl_counters* out);
+/* Fate on the device for every run (per-division streams keyed by each run's
+ * rng_seed, as marl_engine_set_device_fate), or back on the host.  With device
+ * fate a batch tick is one CUDA graph with no host work, and marl_batch_step
+ * synchronises once per call.  Needs the batch surrogate off. */
+marl_status marl_batch_set_device_fate(marl_batch* b, int32_t enable);
 
 /* ---- learned reaction surrogate ----------------------------------------
  * No counterpart in the reference.  A 93 -> 256 -> 256 -> 16 MLP (tanh-form

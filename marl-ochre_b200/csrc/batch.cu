@@ -185,6 +185,19 @@ struct marl_batch {
     bool use_graph = true;
     bool direct_since_change = false;  // a direct tick ran since the last graph invalidation
 
+    // Device fate (marl_batch_set_device_fate): per-run fate buffers, their
+    // FateRun table and scalars; while it is on, populations, tick counters and
+    // completion epochs advance on the device and the host copies are stale
+    // until sync_fate_state.
+    bool device_fate = false;
+    bool fate_stale = false;  // host per-run state behind the device
+    std::vector<FateBuffers> fate;
+    FateRun* d_fate_runs = nullptr;
+    FateScalars* d_fate_scalars = nullptr;  // [runs]
+    FateScalars* h_fate_scalars = nullptr;  // pinned [runs]
+    uint32_t max_cap = 0;
+    cudaGraphExec_t fate_graph[2] = {nullptr, nullptr};
+
     WorkerPool pool;
 
     uint64_t h2d = 0, d2h = 0, launches = 0, ticks = 0;
@@ -212,6 +225,10 @@ struct marl_batch {
 namespace {
 
 void invalidate_graphs(marl_batch* b) {
+    for (auto& g : b->fate_graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
     for (auto& g : b->graph)
         if (g) {
             cudaGraphExecDestroy(g);
@@ -230,11 +247,12 @@ void batch_free(marl_batch* b) {
             if (q) cudaFree(q);
         free_table(r.t);
     }
-    void* dev[] = {b->d_runs, b->d_maps, b->d_diff_items, b->d_light_items, b->d_rb, b->d_edit, b->d_records,
+    for (auto& f : b->fate) free_fate(f);
+    void* dev[] = {b->d_fate_runs, b->d_fate_scalars, b->d_runs, b->d_maps, b->d_diff_items, b->d_light_items, b->d_rb, b->d_edit, b->d_records,
                    b->surr_xt, b->surr_pred, b->surr_x, b->surr_status, b->surr_err, b->surr_counters};
     for (void* p : dev)
         if (p) cudaFree(p);
-    void* host[] = {b->h_runs, b->h_rb, b->h_edit, b->h_records};
+    void* host[] = {b->h_runs, b->h_rb, b->h_edit, b->h_records, b->h_fate_scalars};
     for (void* p : host)
         if (p) cudaFreeHost(p);
     for (auto* v : {&b->span_pool, &b->spans_pending})
@@ -463,6 +481,8 @@ marl_status collect_errors(marl_batch* b, uint32_t bits) {
     cudaStreamSynchronize(b->stream);
     if (bits & (kErrTimeoutMbar | kErrTimeoutDeps))
         return fail(MARL_ERR_TIMEOUT, "device wait gave up (error bits 0x%x)", bits);
+    if (bits & kErrCapacity) return fail(MARL_ERR_CAPACITY, "a run's cell table is full: births dropped (0x%x)", bits);
+    if (bits & kErrFateChain) return fail(MARL_ERR_STATE, "inconsistent death events in device fate (0x%x)", bits);
     return fail(MARL_ERR_INVALID_INPUT, "device rejected input (error bits 0x%x)", bits);
 }
 
@@ -522,6 +542,196 @@ marl_status apply_edits(marl_batch* b) {
                            &b->d_scalars()->err, b->stream));
     span_end(b, span);
     b->launches += (nh > 0) + (nd > 0) + (nm > 0) + (nb > 0);
+    return MARL_OK;
+}
+
+// ---- device fate ----
+
+// One tick of every run with fate on the device (lib.rs:160-277): populations,
+// first global cell indices and epochs from the previous fate step, schedule,
+// sources + diffusion, light, the cell loop, fate.  Nothing crosses to the
+// host; ends with b->cur flipped by the number of substeps.
+marl_status enqueue_device_fate_tick(marl_batch* b, cudaStream_t s, int cur) {
+    const int n_runs = (int)b->runs.size();
+    CK(launch_batch_population(b->d_runs, n_runs, b->d_fate_runs, s));
+    CK(cudaMemsetAsync(&b->d_scalars()->ticket, 0, 4, s));
+    CK(launch_cell_schedule_batch(b->d_runs, n_runs, b->num_sms, s));
+    const uint32_t S = b->sim.diffusion_substeps;
+    uint32_t* err = &b->d_scalars()->err;
+    if (S == 0) {
+        for (auto& R : b->runs) CK(launch_sources(R.field[cur], R.g, b->fk, s));
+    }
+    for (uint32_t i = 0; i < S; ++i) {
+        CK(launch_diffuse_batch(b->tile, b->d_runs, b->d_maps, b->d_diff_items, b->n_diff_items, b->zc, b->fk, cur,
+                                i == 0 ? 1 : 0, i + 1 == S ? 1 : 0, err, s));
+        cur ^= 1;
+    }
+    CK(launch_light_batch(b->d_runs, b->d_light_items, b->n_light_items, b->fk, cur, S > 0 ? 1 : 0, s));
+    CK(launch_cell_tick_batch(b->d_runs, n_runs, b->d_scalars(), b->ck, cur, b->num_sms, kModePlain, s));
+    CK(launch_fate(b->d_fate_runs, n_runs, b->max_cap, err, b->sim, b->num_sms, s));
+    return MARL_OK;
+}
+
+uint64_t device_fate_tick_launches(const marl_batch* b) {
+    const uint32_t S = b->sim.diffusion_substeps;
+    return 1 + 1 + (S ? S : b->runs.size()) + 1 + 1 + 5;
+}
+
+marl_status launch_device_fate_tick(marl_batch* b) {
+    const int cur = b->cur;
+    if (b->use_graph) {
+        if (!b->fate_graph[cur]) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+            marl_status st = enqueue_device_fate_tick(b, b->capture_stream, cur);
+            cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
+            if (st) {
+                if (g) cudaGraphDestroy(g);
+                return st;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&b->fate_graph[cur], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                b->fate_graph[cur] = nullptr;
+                return cuda_fail(e, "cudaGraphInstantiate");
+            }
+        }
+        CK(cudaGraphLaunch(b->fate_graph[cur], b->stream));
+    } else {
+        marl_status st = enqueue_device_fate_tick(b, b->stream, cur);
+        if (st) return st;
+    }
+    if (b->sim.diffusion_substeps & 1u) b->cur ^= 1;
+    b->launches += device_fate_tick_launches(b);
+    return MARL_OK;
+}
+
+// Synchronises and brings every run's population and counters back to the
+// host (one copy of the scalar array).
+marl_status sync_fate_state(marl_batch* b) {
+    if (!b->fate_stale) return MARL_OK;
+    const size_t bytes = b->runs.size() * sizeof(FateScalars);
+    CK(cudaMemcpyAsync(b->h_fate_scalars, b->d_fate_scalars, bytes, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaMemcpyAsync(b->h_rb, b->d_rb, sizeof(BatchScalars), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    resolve_spans(b);
+    b->d2h += bytes + sizeof(BatchScalars);
+    b->d2h_last += bytes + sizeof(BatchScalars);
+    for (size_t r = 0; r < b->runs.size(); ++r) {
+        BatchRun& R = b->runs[r];
+        const FateScalars& f = b->h_fate_scalars[r];
+        R.n = f.n;
+        R.host.tick = f.tick;
+        R.host.total_div = f.total_div;
+        R.host.total_death = f.total_death;
+        R.host.tick_div = f.placed;
+        R.host.tick_death = f.ndeath;
+    }
+    b->fate_stale = false;
+    return collect_errors(b, b->h_scalars()->err);
+}
+
+marl_status device_fate_steps(marl_batch* b, uint32_t ticks) {
+    b->h2d_last = b->d2h_last = 0;
+    uint32_t done = 0;
+    while (done < ticks) {
+        if (b->epoch == 0xFFFFFFFFu) {  // the next epoch would wrap: clear stale completion epochs
+            marl_status st = sync_fate_state(b);
+            if (st) return st;
+            for (auto& R : b->runs) CK(cudaMemsetAsync(R.t.done, 0, (size_t)R.t.cap * 4, b->stream));
+            b->epoch = 0;
+            fill_desc(b);
+            CK(cudaMemcpyAsync(b->d_runs, b->h_runs, b->runs.size() * sizeof(RunDesc), cudaMemcpyHostToDevice,
+                               b->stream));
+            CK(cudaStreamSynchronize(b->stream));
+        }
+        const uint32_t chunk = std::min<uint32_t>(ticks - done, 0xFFFFFFFFu - b->epoch);
+        const int span = span_begin(b);
+        for (uint32_t t = 0; t < chunk; ++t) {
+            b->epoch += 1;  // the device adds one to every run's epoch at the start of the tick
+            marl_status st = launch_device_fate_tick(b);
+            if (st) return st;
+            b->fate_stale = true;
+            ++b->ticks;
+        }
+        span_end(b, span);
+        done += chunk;
+    }
+    return sync_fate_state(b);
+}
+
+marl_status enable_device_fate(marl_batch* b) {
+    if (b->surr) return fail(MARL_ERR_STATE, "device fate runs with the batch surrogate off");
+    const size_t n_runs = b->runs.size();
+    if (b->fate.empty()) {
+        b->fate.resize(n_runs);
+        CK(cudaMalloc((void**)&b->d_fate_scalars, n_runs * sizeof(FateScalars)));
+        CK(cudaMallocHost((void**)&b->h_fate_scalars, n_runs * sizeof(FateScalars)));
+        CK(cudaMalloc((void**)&b->d_fate_runs, n_runs * sizeof(FateRun)));
+        std::vector<FateRun> fr(n_runs);
+        for (size_t r = 0; r < n_runs; ++r) {
+            BatchRun& R = b->runs[r];
+            CK(alloc_fate(b->fate[r], R.cap, R.g.V(), b->d_fate_scalars + r));
+            fr[r].f = b->fate[r];
+            fr[r].t = R.t;
+            fr[r].g = R.g;
+            fr[r].cmap = R.cmap;
+            fr[r].mask = R.mask;
+            b->max_cap = std::max(b->max_cap, R.cap);
+        }
+        CK(cudaMemcpy(b->d_fate_runs, fr.data(), n_runs * sizeof(FateRun), cudaMemcpyHostToDevice));
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    for (size_t r = 0; r < n_runs; ++r) {
+        const BatchRun& R = b->runs[r];
+        FateScalars& f = b->h_fate_scalars[r];
+        std::memset(&f, 0, sizeof(f));
+        f.seed = R.host.seed;
+        f.tick = R.host.tick;
+        f.total_div = R.host.total_div;
+        f.total_death = R.host.total_death;
+        f.n = R.n;
+        f.placed = (uint32_t)R.host.tick_div;
+        f.ndeath = (uint32_t)R.host.tick_death;
+    }
+    // The population kernel adds one to the epoch at the start of each tick.
+    fill_desc(b);
+    CK(cudaMemcpyAsync(b->d_fate_scalars, b->h_fate_scalars, n_runs * sizeof(FateScalars), cudaMemcpyHostToDevice,
+                       b->stream));
+    CK(cudaMemcpyAsync(b->d_runs, b->h_runs, n_runs * sizeof(RunDesc), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    b->h2d += n_runs * (sizeof(FateScalars) + sizeof(RunDesc));
+    b->device_fate = true;
+    b->fate_stale = false;
+    return MARL_OK;
+}
+
+// Back to host fate: each run's host side adopts its device cell vector (its
+// sequential stream continues where it stood).
+marl_status disable_device_fate(marl_batch* b) {
+    marl_status st = sync_fate_state(b);
+    if (st) return st;
+    std::vector<marl_cell> cells;
+    for (size_t r = 0; r < b->runs.size(); ++r) {
+        BatchRun& R = b->runs[r];
+        cells.resize(std::max<uint32_t>(R.n, 1));
+        if (R.n) {
+            if ((st = ensure_records(b, R.n))) return st;
+            CK(launch_cells_to_records(R.t, R.n, b->d_records, b->stream));
+            CK(cudaMemcpyAsync(b->h_records, b->d_records, (size_t)R.n * sizeof(marl_cell), cudaMemcpyDeviceToHost,
+                               b->stream));
+            CK(cudaStreamSynchronize(b->stream));
+            std::memcpy(cells.data(), b->h_records, (size_t)R.n * sizeof(marl_cell));
+            b->d2h += (size_t)R.n * sizeof(marl_cell);
+        }
+        const uint64_t tick = R.host.tick, td = R.host.total_div, tx = R.host.total_death, d1 = R.host.tick_div,
+                       x1 = R.host.tick_death;
+        R.host.adopt(cells.data(), R.n);
+        R.host.tick = tick, R.host.total_div = td, R.host.total_death = tx, R.host.tick_div = d1,
+        R.host.tick_death = x1;
+    }
+    b->device_fate = false;
     return MARL_OK;
 }
 
@@ -814,8 +1024,17 @@ marl_status marl_batch_set_graph(marl_batch* b, int32_t use_graph) {
     return MARL_OK;
 }
 
+marl_status marl_batch_set_device_fate(marl_batch* b, int32_t enable) {
+    if (!b) return fail(MARL_ERR_INVALID_INPUT, "null batch");
+    const bool on = enable != 0;
+    if (on == b->device_fate) return MARL_OK;
+    return on ? enable_device_fate(b) : disable_device_fate(b);
+}
+
 marl_status marl_batch_set_surrogate(marl_batch* b, marl_surrogate* s, int32_t mode, float tol) {
     if (!b) return fail(MARL_ERR_INVALID_INPUT, "null batch");
+    if (mode != MARL_SURR_OFF && b->device_fate)
+        return fail(MARL_ERR_STATE, "the batch surrogate runs with host fate (device fate is on)");
     if (mode != MARL_SURR_OFF && mode != MARL_SURR_GATED && mode != MARL_SURR_TRUSTED)
         return fail(MARL_ERR_INVALID_INPUT, "batch surrogate mode must be OFF, GATED or TRUSTED");
     if (mode != MARL_SURR_OFF && (!s || !s->prepared))
@@ -860,6 +1079,7 @@ marl_status marl_batch_surrogate_counters(marl_batch* b, marl_surrogate_counters
 
 marl_status marl_batch_step(marl_batch* b, uint32_t ticks) {
     if (!b) return fail(MARL_ERR_INVALID_INPUT, "null batch");
+    if (b->device_fate) return device_fate_steps(b, ticks);
     for (uint32_t t = 0; t < ticks; ++t) {
         marl_status st = step_once(b);
         if (st) return st;
@@ -876,9 +1096,11 @@ marl_status marl_batch_run_count(marl_batch* b, uint32_t* n) {
 marl_status marl_batch_stats_get(marl_batch* b, uint32_t run, marl_engine_stats* s) {
     if (!b || !s) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     if (run >= b->runs.size()) return fail(MARL_ERR_INVALID_INPUT, "run %u of %zu", run, b->runs.size());
+    marl_status st = sync_fate_state(b);
+    if (st) return st;
     const HostRun& h = b->runs[run].host;
     s->tick = h.tick;
-    s->population = h.cells.size();
+    s->population = b->device_fate ? b->runs[run].n : h.cells.size();
     s->total_divisions = h.total_div;
     s->total_deaths = h.total_death;
     s->tick_divisions = h.tick_div;
@@ -892,6 +1114,8 @@ marl_status marl_batch_stats_get(marl_batch* b, uint32_t run, marl_engine_stats*
 marl_status marl_batch_get_cells(marl_batch* b, uint32_t run, marl_cell* out, uint32_t cap, uint32_t* n_out) {
     if (!b || !n_out || (cap && !out)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
     if (run >= b->runs.size()) return fail(MARL_ERR_INVALID_INPUT, "run %u of %zu", run, b->runs.size());
+    marl_status sf = sync_fate_state(b);
+    if (sf) return sf;
     BatchRun& R = b->runs[run];
     *n_out = R.n;
     if (R.n > cap) return fail(MARL_ERR_CAPACITY, "%u cells, buffer holds %u", R.n, cap);

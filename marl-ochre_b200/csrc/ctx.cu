@@ -156,6 +156,7 @@ void ctx_free(marl_ctx* c) {
         if (p) cudaFreeHost(p);
     free_table(c->t);
     free_fate(c->fate);
+    if (c->d_fate_run) cudaFree(c->d_fate_run);
     for (auto* v : {&c->span_pool, &c->spans_pending})
         for (auto& s : *v) {
             cudaEventDestroy(s.a);

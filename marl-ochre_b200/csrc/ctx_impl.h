@@ -64,6 +64,7 @@ struct marl_ctx {
     // Device fate (fate.cu).  While n_on_device is set the population lives in
     // fate.fs->n and `n` above is stale; sync_population brings it back.
     marl::FateBuffers fate{};
+    marl::FateRun* d_fate_run = nullptr;  // device copy of this context's FateRun
     bool fate_ready = false;
     bool n_on_device = false;
 

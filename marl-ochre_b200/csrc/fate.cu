@@ -34,6 +34,7 @@
 // death, so a chain has at most as many steps as there are levels.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -57,16 +58,6 @@ uint32_t fate_blocks(uint32_t cap) { return (cap + kFateChunk - 1) / kFateChunk;
 
 // crates/marl-sim/src/spatial.rs:8-15 (FACE order)
 __constant__ int c_fate_face[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-
-struct FateArgs {
-    FateBuffers f;
-    CellTable t;
-    Grid g;
-    int32_t* cmap;
-    uint8_t* mask;
-    uint32_t* err;
-    marl_sim_params sim;
-};
 
 __device__ __forceinline__ size_t vox_of(uint32_t P, const Grid& g) {
     return ((size_t)pos_z(P) * g.Y + pos_y(P)) * g.X + pos_x(P);
@@ -132,28 +123,29 @@ __device__ __forceinline__ uint32_t packed_counts(const uint8_t e[8]) {
     return c;
 }
 
-__global__ void __launch_bounds__(kFateThreads) k_fate_count(const uint8_t* __restrict__ ev,
-                                                             const FateScalars* __restrict__ fs,
-                                                             uint32_t* __restrict__ blk) {
+// Grid (chunks, runs): block (x, r) counts the Division and Death events of
+// run r's cells [2048 x, 2048 x + 2048).
+__global__ void __launch_bounds__(kFateThreads) k_fate_count(const FateRun* __restrict__ runs) {
     __shared__ uint32_t wb[33];
-    const uint32_t n = fs->n;
+    const FateRun& R = runs[blockIdx.y];
+    const uint32_t n = R.f.fs->n;
+    if (blockIdx.x * kFateChunk >= n) return;
     const uint32_t first = blockIdx.x * kFateChunk + threadIdx.x * kFatePerThread;
     uint8_t e[8];
-    load_events8(ev, first, n, e);
+    load_events8(R.t.events, first, n, e);
     const uint32_t tot = block_sum(packed_counts(e), wb);
-    if (threadIdx.x == 0) blk[blockIdx.x] = tot;
+    if (threadIdx.x == 0) R.f.blk[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(kFateThreads) k_fate_scatter(const uint8_t* __restrict__ ev, FateScalars* fs,
-                                                               const uint32_t* __restrict__ blk,
-                                                               uint32_t* __restrict__ div_list,
-                                                               uint32_t* __restrict__ death_list) {
+// Same grid: the chunk's events into the run's ascending Division and Death lists.
+__global__ void __launch_bounds__(kFateThreads) k_fate_scatter(const FateRun* __restrict__ runs) {
     __shared__ uint32_t wb[33];
-    const uint32_t n = fs->n;
-    // Offsets of this block: Division and Death counts of the blocks before it.
-    uint32_t od = 0, ox = 0;
+    const FateRun& R = runs[blockIdx.y];
+    const uint32_t n = R.f.fs->n;
+    if (blockIdx.x * kFateChunk >= n) return;
+    uint32_t od = 0, ox = 0;  // Division and Death counts of the chunks before this one
     for (uint32_t b = threadIdx.x; b < blockIdx.x; b += kFateThreads) {
-        const uint32_t v = blk[b];
+        const uint32_t v = R.f.blk[b];
         od += v & 0xFFFFu;
         ox += v >> 16;
     }
@@ -161,21 +153,14 @@ __global__ void __launch_bounds__(kFateThreads) k_fate_scatter(const uint8_t* __
     ox = block_sum(ox, wb);
     const uint32_t first = blockIdx.x * kFateChunk + threadIdx.x * kFatePerThread;
     uint8_t e[8];
-    load_events8(ev, first, n, e);
+    load_events8(R.t.events, first, n, e);
     uint32_t tot;
     const uint32_t ex = block_scan_excl(packed_counts(e), wb, tot);
     uint32_t pd = od + (ex & 0xFFFFu), px = ox + (ex >> 16);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        if (e[i] == MARL_EVENT_DIVISION) div_list[pd++] = first + i;
-        else if (e[i] == MARL_EVENT_DEATH) death_list[px++] = first + i;
-    }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
-        const uint32_t ndeath = ox + (tot >> 16);
-        fs->ndiv = od + (tot & 0xFFFFu);
-        fs->ndeath = ndeath;
-        fs->n_old = n;
-        fs->n1 = n - ndeath;
+        if (e[i] == MARL_EVENT_DIVISION) R.f.div_list[pd++] = first + i;
+        else if (e[i] == MARL_EVENT_DEATH) R.f.death_list[px++] = first + i;
     }
 }
 
@@ -203,27 +188,42 @@ __device__ __forceinline__ bool place_daughter(uint32_t P, const int32_t* __rest
     return true;
 }
 
-__global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_constant__ FateArgs a) {
+// One block per run.
+__global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const FateRun* __restrict__ runs,
+                                                                  const __grid_constant__ marl_sim_params sim,
+                                                                  uint32_t* err_out) {
     __shared__ uint32_t wb[33];
     __shared__ uint32_t s_win, s_placed, s_run, s_levels, s_err;
-    FateScalars* fs = a.f.fs;
-    const uint32_t n = fs->n_old, n1 = fs->n1, ndiv = fs->ndiv, ndeath = fs->ndeath;
-    const unsigned long long seed = fs->seed, tick = fs->tick;
-    const CellTable& t = a.t;
-    const Grid g = a.g;
+    const FateRun& R = runs[blockIdx.x];
+    const FateBuffers& F = R.f;
+    FateScalars* fs = F.fs;
+    const CellTable& t = R.t;
+    const Grid g = R.g;
     const uint32_t cap = t.cap;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t n = fs->n;
+    const unsigned long long seed = fs->seed, tick = fs->tick;
+
+    // Totals of the compaction.
+    uint32_t part = 0;
+    const uint32_t chunks = (n + kFateChunk - 1) / kFateChunk;
+    for (uint32_t b = tid; b < chunks; b += nthr) part += F.blk[b] & 0xFFFFu;
+    const uint32_t ndiv = block_sum(part, wb);
+    part = 0;
+    for (uint32_t b = tid; b < chunks; b += nthr) part += F.blk[b] >> 16;
+    const uint32_t ndeath = block_sum(part, wb);
+    const uint32_t n1 = n - ndeath;
     if (tid == 0) s_win = s_placed = s_run = s_err = 0;
 
     // A. Placement on the cell map as it stood before the step, and claims.
-    const long long dist = (long long)a.sim.division_neighbor_distance;
+    const long long dist = (long long)sim.division_neighbor_distance;
     for (uint32_t k = tid; k < ndiv; k += nthr) {
-        const uint32_t p = a.f.div_list[k];
+        const uint32_t p = F.div_list[k];
         fate::Stream r(fate::stream_key(seed, tick, p));
         uint32_t target = 0;
-        const bool ok = place_daughter(t.pos[p], a.cmap, g, dist, r, target);
-        a.f.div_info[k] = make_uint2(target, r.draws | (ok ? kPlacedBit : 0u));
-        if (ok) atomicMin(&a.f.claim[vox_of(target, g)], k);
+        const bool ok = place_daughter(t.pos[p], R.cmap, g, dist, r, target);
+        F.div_info[k] = make_uint2(target, r.draws | (ok ? kPlacedBit : 0u));
+        if (ok) atomicMin(&F.claim[vox_of(target, g)], k);
     }
     __syncthreads();
 
@@ -234,20 +234,20 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
         const uint32_t k = base + tid;
         uint32_t flags = 0;  // won | placed << 16
         if (k < ndiv) {
-            const uint2 info = a.f.div_info[k];
-            if (info.y & kPlacedBit) flags = (1u << 16) | (a.f.claim[vox_of(info.x, g)] == k ? 1u : 0u);
+            const uint2 info = F.div_info[k];
+            if (info.y & kPlacedBit) flags = (1u << 16) | (F.claim[vox_of(info.x, g)] == k ? 1u : 0u);
         }
         uint32_t tot;
         const uint32_t ex = block_scan_excl(flags, wb, tot);
         if (k < ndiv) {
             uint32_t slot = kFateNoSlot;
             if (flags & 1u) {
-                const uint64_t s = (uint64_t)n1 + s_win + (ex & 0xFFFFu);
-                slot = s < cap ? (uint32_t)s : kFateDropped;
+                const uint64_t sl = (uint64_t)n1 + s_win + (ex & 0xFFFFu);
+                slot = sl < cap ? (uint32_t)sl : kFateDropped;
             }
-            a.f.div_slot[k] = slot;
+            F.div_slot[k] = slot;
             if (flags >> 16) {
-                const uint32_t p = a.f.div_list[k];
+                const uint32_t p = F.div_list[k];
 #pragma unroll
                 for (int sp = 0; sp < MARL_M_INT; ++sp) {
                     float& v = t.internal[(size_t)sp * cap + p];
@@ -265,10 +265,10 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
 
     // C. Dead cells leave the cell map (lib.rs:261-262).
     for (uint32_t i = tid; i < ndeath; i += nthr) {
-        const uint32_t P = t.pos[a.f.death_list[i]];
+        const uint32_t P = t.pos[F.death_list[i]];
         const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
-        a.cmap[row * g.X + pos_x(P)] = -1;
-        a.mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
+        R.cmap[row * g.X + pos_x(P)] = -1;
+        R.mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
     }
 
     // D. cnt[o] = deaths in [n1, n1 + o) over the tail [n1, n).
@@ -277,23 +277,23 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
         const uint32_t dead = (o < ndeath && t.events[n1 + o] == MARL_EVENT_DEATH) ? 1u : 0u;
         uint32_t tot;
         const uint32_t ex = block_scan_excl(dead, wb, tot);
-        if (o < ndeath) a.f.cnt[o] = s_run + ex;
+        if (o < ndeath) F.cnt[o] = s_run + ex;
         __syncthreads();
         if (tid == 0) s_run += tot;
         __syncthreads();
     }
     const uint32_t m0 = ndeath - s_run;  // holes below n1 = cells that move
-    if (tid == 0) a.f.cnt[ndeath] = s_run;
+    if (tid == 0) F.cnt[ndeath] = s_run;
     __syncthreads();
 
     // E. Level boundaries b_k and D(b_{k-1}).
     if (tid == 0) {
         uint32_t L = 0, b = n1, db = 0;
         for (;;) {
-            a.f.lev_b[L] = b;
-            a.f.lev_d[L] = db;
+            F.lev_b[L] = b;
+            F.lev_d[L] = db;
             ++L;
-            const uint32_t Db = m0 + a.f.cnt[b - n1];
+            const uint32_t Db = m0 + F.cnt[b - n1];
             const uint32_t m = Db - db;
             if (m == 0 || L > ndeath + 1) break;
             if (m > n - b) {  // b never passes n for events consistent with the death list
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
     // F. The cell that ends in hole i, and the new slot of every tail survivor.
     const uint32_t L = s_levels;
     for (uint32_t i = tid; i < m0; i += nthr) {
-        const uint32_t h = a.f.death_list[i];
+        const uint32_t h = F.death_list[i];
         uint32_t q = n1 + i;
         uint32_t steps = 0;
         bool bad = false;
@@ -319,13 +319,13 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
             uint32_t lo = 0, hi = L;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (a.f.lev_b[mid] <= q) lo = mid + 1; else hi = mid;
+                if (F.lev_b[mid] <= q) lo = mid + 1; else hi = mid;
             }
             if (++steps > L || lo == 0 || lo >= L) {
                 bad = true;
                 break;
             }
-            const uint32_t nq = a.f.lev_b[lo] + (m0 + a.f.cnt[q - n1]) - a.f.lev_d[lo];
+            const uint32_t nq = F.lev_b[lo] + (m0 + F.cnt[q - n1]) - F.lev_d[lo];
             if (nq >= n || nq < n1) {
                 bad = true;
                 break;
@@ -333,9 +333,9 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
             q = nq;
         }
         if (bad) atomicOr(&s_err, kErrFateChain);
-        a.f.move_dst[i] = h;
-        a.f.move_src[i] = q;
-        a.f.newidx[q - n1] = h;
+        F.move_dst[i] = h;
+        F.move_src[i] = q;
+        F.newidx[q - n1] = h;
     }
     __syncthreads();
 
@@ -345,8 +345,12 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
         const uint32_t births = s_win < room ? s_win : room;
         uint32_t err = s_err;
         if (births < s_win) err |= kErrCapacity;
-        if (err) atomicOr(a.err, err);
+        if (err) atomicOr(err_out, err);
         fs->n = n1 + births;
+        fs->n_old = n;
+        fs->n1 = n1;
+        fs->ndiv = ndiv;
+        fs->ndeath = ndeath;
         fs->placed = s_placed;
         fs->births = births;
         fs->moves = m0;
@@ -358,29 +362,34 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const __grid_c
     }
 }
 
-__global__ void __launch_bounds__(256) k_fate_moves(const __grid_constant__ FateArgs a) {
-    const uint32_t moves = a.f.fs->moves;
+// Grid (x, runs): warps of the blocks of run r take its moves in turn.
+__global__ void __launch_bounds__(256) k_fate_moves(const FateRun* __restrict__ runs) {
+    const FateRun& R = runs[blockIdx.y];
+    const uint32_t moves = R.f.fs->moves;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < moves; i += warps)
-        move_one(a.t, a.g, a.cmap, a.f.move_dst[i], a.f.move_src[i], threadIdx.x & 31);
+        move_one(R.t, R.g, R.cmap, R.f.move_dst[i], R.f.move_src[i], threadIdx.x & 31);
 }
 
-__global__ void __launch_bounds__(32 * kFateBirthWarps) k_fate_births(const __grid_constant__ FateArgs a) {
+// Grid (x, runs): one warp per division of run r.
+__global__ void __launch_bounds__(32 * kFateBirthWarps) k_fate_births(const FateRun* __restrict__ runs,
+                                                                      const __grid_constant__ marl_sim_params sim) {
     __shared__ __align__(16) marl_cell rec[kFateBirthWarps];
-    const FateScalars* fs = a.f.fs;
+    const FateRun& R = runs[blockIdx.y];
+    const FateScalars* fs = R.f.fs;
     const uint32_t ndiv = fs->ndiv, n1 = fs->n1;
     const unsigned long long seed = fs->seed, tick = fs->key_tick;
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     for (uint32_t k = blockIdx.x * kFateBirthWarps + w; k < ndiv; k += gridDim.x * kFateBirthWarps) {
-        const uint32_t slot = a.f.div_slot[k];
+        const uint32_t slot = R.f.div_slot[k];
         if (slot == kFateNoSlot) continue;
-        const uint2 info = a.f.div_info[k];
-        if (l == 0) a.f.claim[vox_of(info.x, a.g)] = 0xFFFFFFFFu;  // the winner releases its voxel's claim
+        const uint2 info = R.f.div_info[k];
+        if (l == 0) R.f.claim[vox_of(info.x, R.g)] = 0xFFFFFFFFu;  // the winner releases its voxel's claim
         if (slot == kFateDropped) continue;
-        const uint32_t p = a.f.div_list[k];
-        const uint32_t pn = p < n1 ? p : a.f.newidx[p - n1];
+        const uint32_t p = R.f.div_list[k];
+        const uint32_t pn = p < n1 ? p : R.f.newidx[p - n1];
         marl_cell& c = rec[w];
-        read_record_warp(a.t, pn, c);
+        read_record_warp(R.t, pn, c);
         __syncwarp();
         if (l == 0) {
             fate::Stream r(fate::stream_key(seed, tick, p));
@@ -391,11 +400,35 @@ __global__ void __launch_bounds__(32 * kFateBirthWarps) k_fate_births(const __gr
             c.age = 0;
             c.prep_remaining = 0;
             c.lineage_id = r.u64();
-            fate::mutate_ruleset(c.ruleset, r, a.sim);
+            fate::mutate_ruleset(c.ruleset, r, sim);
         }
         __syncwarp();
-        write_record_warp(a.t, a.g, a.cmap, a.mask, slot, c);
+        write_record_warp(R.t, R.g, R.cmap, R.mask, slot, c);
         __syncwarp();
+    }
+}
+
+// Batch: every run's population and first global cell index from its fate
+// scalars, and the next tick's completion epoch (one block).
+__global__ void __launch_bounds__(1024) k_batch_population(RunDesc* __restrict__ runs, int n_runs,
+                                                           const FateRun* __restrict__ fr) {
+    __shared__ uint32_t wb[33];
+    __shared__ uint32_t s_base;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (int base = 0; base < n_runs; base += blockDim.x) {
+        const int r = base + (int)threadIdx.x;
+        const uint32_t n = r < n_runs ? fr[r].f.fs->n : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_scan_excl(n, wb, tot);
+        if (r < n_runs) {
+            runs[r].n = n;
+            runs[r].cell_base = s_base + ex;
+            runs[r].epoch = runs[r].epoch + 1u;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += tot;
+        __syncthreads();
     }
 }
 
@@ -427,13 +460,17 @@ __global__ void k_stream_ln(const double* __restrict__ x, uint32_t n, double* __
 
 // ----------------------------------------------------------- host side ---
 
-cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels) {
+cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels, FateScalars* fs_external) {
     f = FateBuffers{};
     cudaError_t e;
+    if (fs_external) {
+        f.fs = fs_external;
+        f.own_fs = false;
+    }
 #define A(field, type, count)                                                               \
     if ((e = cudaMalloc((void**)&f.field, sizeof(type) * (size_t)(count))) != cudaSuccess) \
         return e;
-    A(fs, FateScalars, 1);
+    if (!fs_external) A(fs, FateScalars, 1);
     A(blk, uint32_t, fate_blocks(cap));
     A(div_list, uint32_t, cap);
     A(death_list, uint32_t, cap);
@@ -447,12 +484,12 @@ cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels) {
     A(newidx, uint32_t, cap);
     A(claim, uint32_t, voxels);
 #undef A
-    if ((e = cudaMemset(f.fs, 0, sizeof(FateScalars))) != cudaSuccess) return e;
+    if ((e = cudaMemset(f.fs, 0, sizeof(FateScalars))) != cudaSuccess) return e;  // zeroed by the owner too
     return cudaMemset(f.claim, 0xFF, voxels * 4);
 }
 
 void free_fate(FateBuffers& f) {
-    void* p[] = {f.fs, f.blk, f.div_list, f.death_list, f.div_info, f.div_slot, f.cnt, f.lev_b, f.lev_d,
+    void* p[] = {f.own_fs ? f.fs : nullptr, f.blk, f.div_list, f.death_list, f.div_info, f.div_slot, f.cnt, f.lev_b, f.lev_d,
                  f.move_dst, f.move_src, f.newidx, f.claim};
     for (void* q : p)
         if (q) cudaFree(q);
@@ -470,22 +507,21 @@ cudaError_t launch_fate_init(FateScalars* fs, unsigned long long seed, unsigned 
     return cudaGetLastError();
 }
 
-cudaError_t launch_fate(const FateBuffers& f, const CellTable& t, const Grid& g, int32_t* cmap, uint8_t* mask,
-                        uint32_t* err, const marl_sim_params& sim, int num_sms, cudaStream_t s) {
-    const uint32_t G = fate_blocks(t.cap);
-    k_fate_count<<<G, kFateThreads, 0, s>>>(t.events, f.fs, f.blk);
-    k_fate_scatter<<<G, kFateThreads, 0, s>>>(t.events, f.fs, f.blk, f.div_list, f.death_list);
-    FateArgs a;
-    a.f = f;
-    a.t = t;
-    a.g = g;
-    a.cmap = cmap;
-    a.mask = mask;
-    a.err = err;
-    a.sim = sim;
-    k_fate_resolve<<<1, kResolveThreads, 0, s>>>(a);
-    k_fate_moves<<<num_sms, 256, 0, s>>>(a);
-    k_fate_births<<<2 * num_sms, 32 * kFateBirthWarps, 0, s>>>(a);
+cudaError_t launch_fate(const FateRun* d_runs, int n_runs, uint32_t max_cap, uint32_t* err, const marl_sim_params& sim,
+                        int num_sms, cudaStream_t s) {
+    if (n_runs <= 0) return cudaSuccess;
+    const dim3 chunks(fate_blocks(max_cap), (unsigned)n_runs);
+    k_fate_count<<<chunks, kFateThreads, 0, s>>>(d_runs);
+    k_fate_scatter<<<chunks, kFateThreads, 0, s>>>(d_runs);
+    k_fate_resolve<<<n_runs, kResolveThreads, 0, s>>>(d_runs, sim, err);
+    const unsigned per_run = (unsigned)std::max(1, 2 * num_sms / n_runs);
+    k_fate_moves<<<dim3(per_run, n_runs), 256, 0, s>>>(d_runs);
+    k_fate_births<<<dim3(per_run, n_runs), 32 * kFateBirthWarps, 0, s>>>(d_runs, sim);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_population(RunDesc* runs, int n_runs, const FateRun* fr, cudaStream_t s) {
+    k_batch_population<<<1, 1024, 0, s>>>(runs, n_runs, fr);
     return cudaGetLastError();
 }
 
@@ -504,6 +540,14 @@ namespace marl {
 marl_status begin_device_population(marl_ctx* c) {
     if (!c->fate_ready) {
         CK(alloc_fate(c->fate, c->t.cap, c->g.V()));
+        FateRun fr;
+        fr.f = c->fate;
+        fr.t = c->t;
+        fr.g = c->g;
+        fr.cmap = c->cmap;
+        fr.mask = c->mask;
+        CK(cudaMalloc((void**)&c->d_fate_run, sizeof(FateRun)));
+        CK(cudaMemcpy(c->d_fate_run, &fr, sizeof(FateRun), cudaMemcpyHostToDevice));
         c->fate_ready = true;
     }
     if (!c->n_on_device) {
@@ -531,7 +575,7 @@ marl_status enqueue_fate(marl_ctx* c) {
     marl_status st = begin_device_population(c);
     if (st) return st;
     c->c4_valid = false;
-    CK(launch_fate(c->fate, c->t, c->g, c->cmap, c->mask, &c->d_hdr->err, c->sim, c->num_sms, c->stream));
+    CK(launch_fate(c->d_fate_run, 1, c->t.cap, &c->d_hdr->err, c->sim, c->num_sms, c->stream));
     c->launches += 5;
     c->schedule_dirty = true;
     return MARL_OK;

@@ -215,17 +215,30 @@ struct FateBuffers {
     uint32_t* move_src = nullptr;    // [cap]
     uint32_t* newidx = nullptr;      // [cap] new slot of the tail survivor at offset o
     uint32_t* claim = nullptr;       // [V] lowest division ordinal claiming the voxel, else 0xFFFFFFFF
+    bool own_fs = true;              // fs allocated with the buffers (else part of a caller's array)
 };
 constexpr uint32_t kFateNoSlot = 0xFFFFFFFFu;
 constexpr uint32_t kFateDropped = 0xFFFFFFFEu;
 uint32_t fate_blocks(uint32_t cap);
-cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels);
+// fs_external (nullable): the run's scalars inside a caller-owned array.
+cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels, FateScalars* fs_external = nullptr);
 void free_fate(FateBuffers& f);
 cudaError_t launch_set_population(FateScalars* fs, uint32_t n, cudaStream_t s);
 cudaError_t launch_fate_init(FateScalars* fs, unsigned long long seed, unsigned long long tick,
                              unsigned long long total_div, unsigned long long total_death, cudaStream_t s);
-// The fate step over the events of the table's first fs->n cells.
-cudaError_t launch_fate(const FateBuffers& f, const CellTable& t, const Grid& g, int32_t* cmap, uint8_t* mask,
-                        uint32_t* err, const marl_sim_params& sim, int num_sms, cudaStream_t s);
+// One run as the fate kernels see it (a device array, pointers fixed).
+struct FateRun {
+    FateBuffers f;
+    CellTable t;
+    Grid g;
+    int32_t* cmap;
+    uint8_t* mask;
+};
+// The fate step of every run in d_runs over the events of its first fs->n
+// cells; max_cap: the largest table capacity among them.
+cudaError_t launch_fate(const FateRun* d_runs, int n_runs, uint32_t max_cap, uint32_t* err, const marl_sim_params& sim,
+                        int num_sms, cudaStream_t s);
+// Batch: runs[r].n and .cell_base from the runs' fate scalars, runs[r].epoch += 1.
+cudaError_t launch_batch_population(RunDesc* runs, int n_runs, const FateRun* fr, cudaStream_t s);
 
 }  // namespace marl

@@ -221,7 +221,7 @@ EXPORTED = [
     "marl_batch_set_surrogate", "marl_batch_surrogate_counters", "marl_surrogate_set_inference",
     "marl_ctx_stats", "marl_ctx_viewer_cells", "marl_write_dump",
     "marl_ctx_fate_init", "marl_ctx_fate", "marl_ctx_fate_stats", "marl_ctx_set_events", "marl_ctx_run_ticks",
-    "marl_fate_stream_probe", "marl_fate_stream_ln", "marl_engine_set_device_fate",
+    "marl_fate_stream_probe", "marl_fate_stream_ln", "marl_engine_set_device_fate", "marl_batch_set_device_fate",
 ]
 
 _lib = None
@@ -327,6 +327,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_fate_stream_probe": (c_int32, [c_uint64, c_uint64, c_uint32, c_uint32, c_float, P, P]),
         "marl_fate_stream_ln": (c_int32, [P, c_uint32, P]),
         "marl_engine_set_device_fate": (c_int32, [P, c_int32]),
+        "marl_batch_set_device_fate": (c_int32, [P, c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -771,6 +772,10 @@ class Batch:
 
     def step(self, ticks: int = 1) -> None:
         _check(self.lib.marl_batch_step(self.h, ticks), "marl_batch_step")
+
+    def set_device_fate(self, enable: bool = True) -> None:
+        """Fate of every run on the device (per-division streams keyed by each run's seed) or on the host."""
+        _check(self.lib.marl_batch_set_device_fate(self.h, 1 if enable else 0), "marl_batch_set_device_fate")
 
     def set_surrogate(self, surrogate: "Surrogate | None", mode: int, tol: float = 1e-3) -> None:
         _check(self.lib.marl_batch_set_surrogate(self.h, surrogate.h if surrogate is not None else None, mode, tol),

@@ -207,3 +207,69 @@ def test_run_ticks_batches_without_sync(marl, oracle_mod):
         assert sa[k] == sb[k], k
     assert a.cells().tobytes() == b.cells().tobytes()
     np.testing.assert_array_equal(a.field(), b.field())
+
+
+BATCH_RUNS = [((24, 24, 16), 3), ((32, 24, 24), 7), ((48, 40, 64), 42), ((40, 36, 32), 11)]
+
+
+def device_fate_engines(marl, p, runs, ticks, switch_at=None):
+    out = []
+    for dims, seed in runs:
+        e = marl.Engine(dims, p, rng_seed=seed, seed_count=30, cell_capacity=1 << 14)
+        if switch_at is None:
+            e.set_device_fate(True)
+            e.step(ticks)
+        else:
+            e.step(switch_at)
+            e.set_device_fate(True)
+            e.step(ticks - switch_at)
+        out.append(e)
+    return out
+
+
+def assert_batch_run_equal(batch, r, eng):
+    bs, es = batch.stats(r), eng.stats()
+    for k in ("tick", "population", "total_divisions", "total_deaths", "tick_divisions", "tick_deaths"):
+        assert bs[k] == es[k], (r, k, bs[k], es[k])
+    assert batch.cells(r).tobytes() == eng.cells().tobytes(), r
+    assert np.array_equal(batch.field(r).view(np.uint32), eng.field().view(np.uint32)), r
+    assert np.array_equal(batch.light(r).view(np.uint32), eng.light().view(np.uint32)), r
+
+
+@pytest.mark.parametrize("substeps,graph", [(10, True), (3, True), (10, False)])
+def test_batch_device_fate_matches_engines(marl, substeps, graph):
+    """Each run of a batch with device fate equals a single engine with device
+    fate, bit for bit (odd substep counts alternate the two captured graphs)."""
+    p = marl.default_params()
+    p.diffusion_substeps = substeps
+    b = marl.Batch(BATCH_RUNS, p, cell_capacity=1 << 14)
+    b.set_graph(graph)
+    b.set_device_fate(True)
+    b.step(25)
+    b.step(15)
+    refs = device_fate_engines(marl, p, BATCH_RUNS, 40)
+    events = 0
+    for r, eng in enumerate(refs):
+        assert_batch_run_equal(b, r, eng)
+        events += b.stats(r)["total_divisions"]
+    assert events > 0
+
+
+def test_batch_switches_fate_modes(marl):
+    """Host fate for 10 ticks, device fate for 20, host fate again: every run
+    equals an engine that switched at the same ticks."""
+    p = marl.default_params()
+    b = marl.Batch(BATCH_RUNS, p, cell_capacity=1 << 14)
+    b.step(10)
+    b.set_device_fate(True)
+    b.step(20)
+    b.set_device_fate(False)
+    b.step(10)
+    for r, (dims, seed) in enumerate(BATCH_RUNS):
+        e = marl.Engine(dims, p, rng_seed=seed, seed_count=30, cell_capacity=1 << 14)
+        e.step(10)
+        e.set_device_fate(True)
+        e.step(20)
+        e.set_device_fate(False)
+        e.step(10)
+        assert_batch_run_equal(b, r, e)
