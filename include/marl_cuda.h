@@ -238,6 +238,11 @@ marl_status marl_ctx_synchronize(marl_ctx* ctx);
  * Every choice gives bit-identical results; only speed differs. */
 marl_status marl_ctx_set_tile(marl_ctx* ctx, int32_t tile, int32_t zc);
 marl_status marl_ctx_get_tile(marl_ctx* ctx, int32_t* tile, int32_t* zc);
+/* Cells per warp of the cell loop (1..32, default 32): a warp takes that many
+ * consecutive cells per ticket and leaves its other lanes idle.  Fewer cells
+ * per warp serialise less work inside a warp along the dependency chains, at
+ * the cost of more warps.  Results do not depend on it. */
+marl_status marl_ctx_set_cell_lanes(marl_ctx* ctx, uint32_t lanes);
 /* Tile autotuner (no reference counterpart): times `reps` substeps of every
  * tile shape / z-chunk candidate on this context's grid with CUDA events and
  * keeps the fastest.  The live field is not modified. */

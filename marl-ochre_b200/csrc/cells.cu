@@ -503,16 +503,16 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
 // maps a ticket (global cell index) to the lane's run view and local index.
 template <int MODE, class Resolve>
 __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts& c, uint32_t total, uint32_t* ticket,
-                                               uint32_t* err, Resolve resolve) {
+                                               uint32_t* err, uint32_t lanes, Resolve resolve) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     for (;;) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(ticket, 32u);
+        if (lane == 0) base = atomicAdd(ticket, lanes);
         base = __shfl_sync(FULL, base, 0);
         if (base >= total) break;
         const uint32_t gi = base + lane;
-        bool pending = gi < total;
+        bool pending = (uint32_t)lane < lanes && gi < total;
         CellRunView v{};
         uint32_t j = 0;
         CellPre pre;
@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constan
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const uint32_t total = a.n_dev ? *a.n_dev : a.n;
-    cell_tick_loop<MODE>(S, a.k, total, a.ticket, a.err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    cell_tick_loop<MODE>(S, a.k, total, a.ticket, a.err, a.lanes, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv};
         j = gi;
     });
@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc*
                                                                   int parity) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    cell_tick_loop<MODE>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    cell_tick_loop<MODE>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, 32u, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         const RunDesc& R = runs[find_run(runs, n_runs, gi)];
         v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv};
         j = gi - R.cell_base;
@@ -1049,7 +1049,7 @@ static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaS
         if (per_sm < 1) per_sm = 1;
         configured_device = dev;
     }
-    const uint32_t warps_needed = (a.n + 31) / 32;
+    const uint32_t warps_needed = (a.n + a.lanes - 1) / a.lanes;
     const uint32_t blocks_needed = (warps_needed + (kTickThreads / 32) - 1) / (kTickThreads / 32);
     // Persistent: never more blocks than can be resident at once, so every
     // ticket holder is running (the dependency waits rely on it).

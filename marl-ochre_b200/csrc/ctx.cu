@@ -212,6 +212,7 @@ CellLaunch cell_launch(marl_ctx* c) {
     a.k = c->ck;
     a.epoch = c->epoch;
     a.ticket = &c->d_hdr->pad[0];
+    a.lanes = c->cell_lanes;
     a.err = &c->d_hdr->err;
     return a;
 }
@@ -518,6 +519,13 @@ marl_status marl_ctx_set_tile(marl_ctx* c, int32_t tile, int32_t zc) {
     if (!plan_diffusion(&p, c->field[0], c->field[1], c->mask, c->g, tile, zc))
         return fail(MARL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     c->plan = p;
+    return MARL_OK;
+}
+
+marl_status marl_ctx_set_cell_lanes(marl_ctx* c, uint32_t lanes) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    if (lanes < 1 || lanes > 32) return fail(MARL_ERR_INVALID_INPUT, "lanes %u outside 1..32", lanes);
+    c->cell_lanes = lanes;
     return MARL_OK;
 }
 

@@ -34,6 +34,7 @@ struct marl_ctx {
     float* c4 = nullptr;       // [z][y][x] species 4 after the last substep of a tick
     bool c4_valid = false;     // c4 equals species 4 of field[cur]
     marl::CellTable t{};
+    uint32_t cell_lanes = 32;  // cells per warp ticket of the cell loop
     uint32_t n = 0;
     uint32_t epoch = 0;
     bool schedule_dirty = true;

@@ -140,6 +140,7 @@ struct CellLaunch {
     CellTable t;
     uint32_t n;                     // cells (an upper bound when n_dev is set)
     const uint32_t* n_dev = nullptr;  // device-resident cell count (device fate), read by the kernels
+    uint32_t lanes = 32;              // cells per warp ticket (1..32)
     Grid g;
     const uint8_t* mask;
     const int32_t* cmap;

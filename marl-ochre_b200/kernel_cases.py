@@ -4,8 +4,9 @@
     python marl-ochre_b200/kernel_cases.py cells [--dims 128 128 64] [--cells 90] [--reps 4]
     python marl-ochre_b200/kernel_cases.py light [--dims 128 128 64] [--reps 4]
     python marl-ochre_b200/kernel_cases.py mlp [--rows 300000] [--reps 4]
-    python marl-ochre_b200/kernel_cases.py engine [--ticks 1000]   (seed-42 default run; one
-        k_cell_tick launch per tick, so `-k regex:k_cell_tick -s <ticks-1> -c 1` captures the last)
+    python marl-ochre_b200/kernel_cases.py engine [--ticks 1000] [--device-fate]   (seed-42 default
+        run; one k_cell_tick launch per tick, so `-k regex:k_cell_tick -s <ticks-1> -c 1` captures
+        the last; with --device-fate the fate step runs on the GPU and all ticks are enqueued at once)
 
 Each case builds a context, uploads seeded synthetic state and runs the kernel
 a few times.  Under `ncu -k regex:<kernel> -s <n> -c 1` that captures one
@@ -95,6 +96,7 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["diffusion", "cells", "light", "mlp", "engine"])
     ap.add_argument("--ticks", type=int, default=1000, help="engine: ticks of the seed-42 default run")
+    ap.add_argument("--device-fate", action="store_true", help="engine: fate on the device")
     ap.add_argument("--rows", type=int, default=300_000, help="mlp: rows (cells) per inference")
     ap.add_argument("--dims", type=int, nargs=3, default=[128, 128, 64])
     ap.add_argument("--tile", type=int, default=-1, help="diffusion tile index (-1: autotune)")
@@ -110,6 +112,8 @@ def main() -> int:
         return mlp_case(a.rows, a.reps, rng)
     if a.case == "engine":
         e = marl.Engine(dims, marl.default_params(), rng_seed=42, seed_count=30, cell_capacity=1 << 20)
+        if a.device_fate:
+            e.set_device_fate(True)
         e.step(a.ticks)
         print(f"engine ok: dims={dims} ticks={a.ticks} stats={e.stats()}")
         return 0

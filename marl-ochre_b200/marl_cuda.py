@@ -199,7 +199,7 @@ LIB_PATH = os.path.join(HERE, "libmarl_cuda.so")
 EXPORTED = [
     "marl_sim_params_default", "marl_last_error", "marl_abi_version",
     "marl_ctx_create", "marl_ctx_destroy", "marl_ctx_set_stream", "marl_ctx_set_params", "marl_ctx_synchronize",
-    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_autotune", "marl_ctx_counters",
+    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_set_cell_lanes", "marl_ctx_autotune", "marl_ctx_counters",
     "marl_upload_field", "marl_download_field", "marl_upload_light", "marl_download_light",
     "marl_upload_cells", "marl_download_cells", "marl_cell_count", "marl_download_occupancy",
     "marl_apply_boundary_sources", "marl_diffuse", "marl_light_update", "marl_cell_phase", "marl_tick",
@@ -247,6 +247,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_synchronize": (c_int32, [P]),
         "marl_ctx_set_tile": (c_int32, [P, c_int32, c_int32]),
         "marl_ctx_get_tile": (c_int32, [P, POINTER(c_int32), POINTER(c_int32)]),
+        "marl_ctx_set_cell_lanes": (c_int32, [P, c_uint32]),
         "marl_ctx_autotune": (c_int32, [P, c_int32, POINTER(c_float)]),
         "marl_ctx_counters": (c_int32, [P, POINTER(Counters)]),
         "marl_upload_field": (c_int32, [P, P]),
