@@ -410,43 +410,77 @@ __global__ void __launch_bounds__(kDiffTX* TY)
 // crates/marl-field/src/light.rs:29-59.  The running intensity of a column is
 // an exclusive product with a floor to zero; the floor makes it
 // non-associative, so each column is multiplied strictly in z order.  A block
-// covers 32 columns of one y row: all 256 threads first evaluate the
-// attenuation factors of a 64-plane segment in parallel (exp in double,
-// rounded to float: the reference calls glibc expf, within 0.502 ulp), then
-// one warp runs the 32 sequential column products through that segment.
+// covers 32 columns of one y row and walks z in 64-plane segments.  The
+// attenuation factors of a segment (exp in double, rounded to float: the
+// reference calls glibc expf, within 0.502 ulp) and its occupancy go to one of
+// two shared buffers; while warp 0 runs the 32 sequential column products
+// through segment s, warps 1-7 load and evaluate segment s+1 into the other
+// buffer.  Each thread issues all its loads of a segment before it uses any.
 constexpr int kLightCols = 32;
 constexpr int kLightSeg = 64;
+constexpr int kLightThreads = 256;
+
+// Factors and occupancy of planes zs .. zs+nz-1 into buffer (fac, occ), by
+// the NT threads t = 0 .. NT-1.
+template <int NT>
+__device__ __forceinline__ void light_fill(const float* __restrict__ c4, const float* __restrict__ field,
+                                           const uint8_t* __restrict__ mask, const Grid& g, const FieldConsts& k,
+                                           int x0, int y, int zs, int nz, int t, float (*fac)[kLightCols],
+                                           uint8_t (*occ)[kLightCols]) {
+    constexpr int kItems = (kLightSeg * kLightCols + NT - 1) / NT;
+    const int pitch = mask_pitch(g.X);
+    const float neg_chem = -k.chemical_absorption;
+    float a[kItems];
+    uint8_t o[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const int i = t + j * NT, zz = i / kLightCols, xg = x0 + i % kLightCols;
+        a[j] = 0.0f;
+        o[j] = 0;
+        if (zz < nz && xg < g.X) {
+            const size_t v = ((size_t)(zs + zz) * g.Y + y) * g.X + xg;
+            a[j] = c4 ? c4[v] : field[v * 12 + 4];
+            o[j] = mask[((size_t)(zs + zz) * g.Y + y) * pitch + xg];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const int i = t + j * NT, zz = i / kLightCols, xi = i % kLightCols;
+        if (zz < nz && x0 + xi < g.X) {
+            fac[zz][xi] = (float)exp((double)(neg_chem * a[j]));
+            occ[zz][xi] = o[j];
+        }
+    }
+}
 
 __device__ __forceinline__ void light_columns(const float* __restrict__ c4, const float* __restrict__ field,
                                               const uint8_t* __restrict__ mask, float* __restrict__ light,
                                               const Grid g, const FieldConsts& k, const int x0, const int y) {
-    __shared__ float fac[kLightSeg][kLightCols];
-    __shared__ uint8_t occ[kLightSeg][kLightCols];
+    __shared__ float fac[2][kLightSeg][kLightCols];
+    __shared__ uint8_t occ[2][kLightSeg][kLightCols];
     const int tid = threadIdx.x, lane = tid & 31;
-    const int pitch = mask_pitch(g.X);
-    const float neg_chem = -k.chemical_absorption;
+    const int nseg = (g.Z + kLightSeg - 1) / kLightSeg;
     float inten = k.surface_intensity;
-    for (int zs = 0; zs < g.Z; zs += kLightSeg) {
-        const int nz = min(kLightSeg, g.Z - zs);
-        for (int i = tid; i < nz * kLightCols; i += 256) {
-            const int zz = i / kLightCols, xi = i % kLightCols, xg = x0 + xi;
-            if (xg < g.X) {
-                const size_t v = ((size_t)(zs + zz) * g.Y + y) * g.X + xg;
-                const float a = c4 ? c4[v] : field[v * 12 + 4];
-                fac[zz][xi] = (float)exp((double)(neg_chem * a));
-                occ[zz][xi] = mask[((size_t)(zs + zz) * g.Y + y) * pitch + xg];
+    light_fill<kLightThreads>(c4, field, mask, g, k, x0, y, 0, min(kLightSeg, g.Z), tid, fac[0], occ[0]);
+    __syncthreads();
+    for (int s = 0; s < nseg; ++s) {
+        const int zs = s * kLightSeg, nz = min(kLightSeg, g.Z - zs);
+        const int buf = s & 1;
+        if (tid < 32) {
+            if (x0 + lane < g.X) {
+                float* out = light + ((size_t)zs * g.Y + y) * g.X + x0 + lane;
+                const size_t plane = (size_t)g.X * g.Y;
+                for (int zz = 0; zz < nz; ++zz) {
+                    out[zz * plane] = inten;
+                    if (occ[buf][zz][lane]) inten *= k.cell_factor;
+                    inten *= fac[buf][zz][lane];
+                    if (inten < k.light_floor) inten = 0.0f;
+                }
             }
-        }
-        __syncthreads();
-        if (tid < 32 && x0 + lane < g.X) {
-            float* out = light + ((size_t)zs * g.Y + y) * g.X + x0 + lane;
-            const size_t plane = (size_t)g.X * g.Y;
-            for (int zz = 0; zz < nz; ++zz) {
-                out[zz * plane] = inten;
-                if (occ[zz][lane]) inten *= k.cell_factor;
-                inten *= fac[zz][lane];
-                if (inten < k.light_floor) inten = 0.0f;
-            }
+        } else if (s + 1 < nseg) {
+            const int zn = zs + kLightSeg;
+            light_fill<kLightThreads - 32>(c4, field, mask, g, k, x0, y, zn, min(kLightSeg, g.Z - zn), tid - 32,
+                                           fac[buf ^ 1], occ[buf ^ 1]);
         }
         __syncthreads();
     }
