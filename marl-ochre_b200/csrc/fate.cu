@@ -15,11 +15,11 @@
 // Kernels of one step (n = cells at its start, all counts device-resident):
 //   k_fate_count / k_fate_scatter   ordered compaction of Division and Death
 //                                   events into ascending lists (2048 cells per block)
-//   k_fate_resolve (one block)      placement + voxel claims (atomicMin of the
-//                                   division ordinal), birth slots in division
-//                                   order, halving, dead voxels cleared, the
-//                                   swap_remove permutation, new population
-//   k_fate_moves                    one warp per swap_remove move
+//   k_fate_resolve (two blocks)     block 0: placement + voxel claims (atomicMin
+//                                   of the division ordinal), birth slots in
+//                                   division order, halving, new population;
+//                                   block 1: the swap_remove permutation
+//   k_fate_moves                    dead voxels cleared; one warp per swap_remove move
 //   k_fate_births                   one warp per daughter: gather the parent's
 //                                   row, draw + mutate on one lane, write the slot
 //
@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(kFateThreads) k_fate_scatter(const FateRun* __
     __shared__ uint32_t wb[33];
     const FateRun& R = runs[blockIdx.y];
     const uint32_t n = R.f.fs->n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) R.f.fs->n_old = n;  // the population the step starts from
     if (blockIdx.x * kFateChunk >= n) return;
     uint32_t od = 0, ox = 0;  // Division and Death counts of the chunks before this one
     for (uint32_t b = threadIdx.x; b < blockIdx.x; b += kFateThreads) {
@@ -188,21 +189,23 @@ __device__ __forceinline__ bool place_daughter(uint32_t P, const int32_t* __rest
     return true;
 }
 
-// One block per run.
+// Grid (2, runs).  Block 0 of run r places the daughters, picks the births
+// and halves the placed parents; block 1 works out the swap_remove
+// permutation.  Neither touches what the other reads, so they run side by
+// side.
 __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const FateRun* __restrict__ runs,
                                                                   const __grid_constant__ marl_sim_params sim,
                                                                   uint32_t* err_out) {
     __shared__ uint32_t wb[33];
     __shared__ uint32_t s_win, s_placed, s_run, s_levels, s_err;
-    const FateRun& R = runs[blockIdx.x];
+    const FateRun& R = runs[blockIdx.y];
     const FateBuffers& F = R.f;
     FateScalars* fs = F.fs;
     const CellTable& t = R.t;
     const Grid g = R.g;
     const uint32_t cap = t.cap;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
-    const uint32_t n = fs->n;
-    const unsigned long long seed = fs->seed, tick = fs->tick;
+    const uint32_t n = fs->n_old;
 
     // Totals of the compaction.
     uint32_t part = 0;
@@ -214,62 +217,81 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const FateRun*
     const uint32_t ndeath = block_sum(part, wb);
     const uint32_t n1 = n - ndeath;
     if (tid == 0) s_win = s_placed = s_run = s_err = 0;
-
-    // A. Placement on the cell map as it stood before the step, and claims.
-    const long long dist = (long long)sim.division_neighbor_distance;
-    for (uint32_t k = tid; k < ndiv; k += nthr) {
-        const uint32_t p = F.div_list[k];
-        fate::Stream r(fate::stream_key(seed, tick, p));
-        uint32_t target = 0;
-        const bool ok = place_daughter(t.pos[p], R.cmap, g, dist, r, target);
-        F.div_info[k] = make_uint2(target, r.draws | (ok ? kPlacedBit : 0u));
-        if (ok) atomicMin(&F.claim[vox_of(target, g)], k);
-    }
     __syncthreads();
 
-    // B. A daughter is born when its division holds the lowest ordinal among
-    // the claims on its voxel; slots follow division order.  Every placed
-    // parent is halved, whether or not its daughter survives the collision.
-    for (uint32_t base = 0; base < ndiv; base += nthr) {
-        const uint32_t k = base + tid;
-        uint32_t flags = 0;  // won | placed << 16
-        if (k < ndiv) {
-            const uint2 info = F.div_info[k];
-            if (info.y & kPlacedBit) flags = (1u << 16) | (F.claim[vox_of(info.x, g)] == k ? 1u : 0u);
+    if (blockIdx.x == 0) {
+        const unsigned long long seed = fs->seed, tick = fs->tick;
+        // A. Placement on the cell map as it stood before the step, and claims.
+        const long long dist = (long long)sim.division_neighbor_distance;
+        for (uint32_t k = tid; k < ndiv; k += nthr) {
+            const uint32_t p = F.div_list[k];
+            fate::Stream r(fate::stream_key(seed, tick, p));
+            uint32_t target = 0;
+            const bool ok = place_daughter(t.pos[p], R.cmap, g, dist, r, target);
+            F.div_info[k] = make_uint2(target, r.draws | (ok ? kPlacedBit : 0u));
+            if (ok) atomicMin(&F.claim[vox_of(target, g)], k);
         }
-        uint32_t tot;
-        const uint32_t ex = block_scan_excl(flags, wb, tot);
-        if (k < ndiv) {
-            uint32_t slot = kFateNoSlot;
-            if (flags & 1u) {
-                const uint64_t sl = (uint64_t)n1 + s_win + (ex & 0xFFFFu);
-                slot = sl < cap ? (uint32_t)sl : kFateDropped;
+        __syncthreads();
+
+        // B. A daughter is born when its division holds the lowest ordinal
+        // among the claims on its voxel; slots follow division order.  Every
+        // placed parent is halved, whether or not its daughter survives the
+        // collision.
+        for (uint32_t base = 0; base < ndiv; base += nthr) {
+            const uint32_t k = base + tid;
+            uint32_t flags = 0;  // won | placed << 16
+            if (k < ndiv) {
+                const uint2 info = F.div_info[k];
+                if (info.y & kPlacedBit) flags = (1u << 16) | (F.claim[vox_of(info.x, g)] == k ? 1u : 0u);
             }
-            F.div_slot[k] = slot;
-            if (flags >> 16) {
-                const uint32_t p = F.div_list[k];
+            uint32_t tot;
+            const uint32_t ex = block_scan_excl(flags, wb, tot);
+            if (k < ndiv) {
+                uint32_t slot = kFateNoSlot;
+                if (flags & 1u) {
+                    const uint64_t sl = (uint64_t)n1 + s_win + (ex & 0xFFFFu);
+                    slot = sl < cap ? (uint32_t)sl : kFateDropped;
+                }
+                F.div_slot[k] = slot;
+                if (flags >> 16) {
+                    const uint32_t p = F.div_list[k];
 #pragma unroll
-                for (int sp = 0; sp < MARL_M_INT; ++sp) {
-                    float& v = t.internal[(size_t)sp * cap + p];
-                    v = v * 0.5f;
+                    for (int sp = 0; sp < MARL_M_INT; ++sp) {
+                        float& v = t.internal[(size_t)sp * cap + p];
+                        v = v * 0.5f;
+                    }
                 }
             }
+            __syncthreads();
+            if (tid == 0) {
+                s_win += tot & 0xFFFFu;
+                s_placed += tot >> 16;
+            }
+            __syncthreads();
         }
-        __syncthreads();
+
+        // Population and counters.
         if (tid == 0) {
-            s_win += tot & 0xFFFFu;
-            s_placed += tot >> 16;
+            const uint32_t room = cap - n1;
+            const uint32_t births = s_win < room ? s_win : room;
+            if (births < s_win) atomicOr(err_out, kErrCapacity);
+            fs->n = n1 + births;
+            fs->n1 = n1;
+            fs->ndiv = ndiv;
+            fs->ndeath = ndeath;
+            fs->placed = s_placed;
+            fs->births = births;
+            fs->key_tick = tick;
+            fs->tick = tick + 1;
+            fs->total_div += s_placed;
+            fs->total_death += ndeath;
         }
-        __syncthreads();
+        return;
     }
 
-    // C. Dead cells leave the cell map (lib.rs:261-262).
-    for (uint32_t i = tid; i < ndeath; i += nthr) {
-        const uint32_t P = t.pos[F.death_list[i]];
-        const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
-        R.cmap[row * g.X + pos_x(P)] = -1;
-        R.mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
-    }
+    // C. Positions of the dying cells, for k_fate_moves to clear their voxels
+    // (lib.rs:261-262) once block 0's placement has read the cell map.
+    for (uint32_t i = tid; i < ndeath; i += nthr) F.dead_pos[i] = t.pos[F.death_list[i]];
 
     // D. cnt[o] = deaths in [n1, n1 + o) over the tail [n1, n).
     for (uint32_t base = 0; base < ndeath; base += nthr) {
@@ -338,33 +360,26 @@ __global__ void __launch_bounds__(kResolveThreads) k_fate_resolve(const FateRun*
         F.newidx[q - n1] = h;
     }
     __syncthreads();
-
-    // G. Population and counters.
     if (tid == 0) {
-        const uint32_t room = cap - n1;
-        const uint32_t births = s_win < room ? s_win : room;
-        uint32_t err = s_err;
-        if (births < s_win) err |= kErrCapacity;
-        if (err) atomicOr(err_out, err);
-        fs->n = n1 + births;
-        fs->n_old = n;
-        fs->n1 = n1;
-        fs->ndiv = ndiv;
-        fs->ndeath = ndeath;
-        fs->placed = s_placed;
-        fs->births = births;
+        if (s_err) atomicOr(err_out, s_err);
         fs->moves = m0;
         fs->levels = L;
-        fs->key_tick = tick;
-        fs->tick = tick + 1;
-        fs->total_div += s_placed;
-        fs->total_death += ndeath;
     }
 }
 
-// Grid (x, runs): warps of the blocks of run r take its moves in turn.
+// Grid (x, runs): the dying cells' voxels are cleared, and warps of the
+// blocks of run r take its moves in turn.  A cleared voxel belongs to a dead
+// cell and a moved cell keeps its own voxel, so the two never meet.
 __global__ void __launch_bounds__(256) k_fate_moves(const FateRun* __restrict__ runs) {
     const FateRun& R = runs[blockIdx.y];
+    const Grid g = R.g;
+    const uint32_t ndeath = R.f.fs->ndeath;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ndeath; i += gridDim.x * blockDim.x) {
+        const uint32_t P = R.f.dead_pos[i];
+        const size_t row = (size_t)pos_z(P) * g.Y + pos_y(P);
+        R.cmap[row * g.X + pos_x(P)] = -1;
+        R.mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
+    }
     const uint32_t moves = R.f.fs->moves;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < moves; i += warps)
@@ -482,6 +497,7 @@ cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels, FateScalars*
     A(move_dst, uint32_t, cap);
     A(move_src, uint32_t, cap);
     A(newidx, uint32_t, cap);
+    A(dead_pos, uint32_t, cap);
     A(claim, uint32_t, voxels);
 #undef A
     if ((e = cudaMemset(f.fs, 0, sizeof(FateScalars))) != cudaSuccess) return e;  // zeroed by the owner too
@@ -490,7 +506,7 @@ cudaError_t alloc_fate(FateBuffers& f, uint32_t cap, size_t voxels, FateScalars*
 
 void free_fate(FateBuffers& f) {
     void* p[] = {f.own_fs ? f.fs : nullptr, f.blk, f.div_list, f.death_list, f.div_info, f.div_slot, f.cnt, f.lev_b, f.lev_d,
-                 f.move_dst, f.move_src, f.newidx, f.claim};
+                 f.move_dst, f.move_src, f.newidx, f.dead_pos, f.claim};
     for (void* q : p)
         if (q) cudaFree(q);
     f = FateBuffers{};
@@ -513,7 +529,7 @@ cudaError_t launch_fate(const FateRun* d_runs, int n_runs, uint32_t max_cap, uin
     const dim3 chunks(fate_blocks(max_cap), (unsigned)n_runs);
     k_fate_count<<<chunks, kFateThreads, 0, s>>>(d_runs);
     k_fate_scatter<<<chunks, kFateThreads, 0, s>>>(d_runs);
-    k_fate_resolve<<<n_runs, kResolveThreads, 0, s>>>(d_runs, sim, err);
+    k_fate_resolve<<<dim3(2, n_runs), kResolveThreads, 0, s>>>(d_runs, sim, err);
     const unsigned per_run = (unsigned)std::max(1, 2 * num_sms / n_runs);
     k_fate_moves<<<dim3(per_run, n_runs), 256, 0, s>>>(d_runs);
     k_fate_births<<<dim3(per_run, n_runs), 32 * kFateBirthWarps, 0, s>>>(d_runs, sim);

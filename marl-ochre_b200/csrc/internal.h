@@ -215,6 +215,7 @@ struct FateBuffers {
     uint32_t* move_dst = nullptr;    // [cap]
     uint32_t* move_src = nullptr;    // [cap]
     uint32_t* newidx = nullptr;      // [cap] new slot of the tail survivor at offset o
+    uint32_t* dead_pos = nullptr;    // [cap] packed positions of the dying cells
     uint32_t* claim = nullptr;       // [V] lowest division ordinal claiming the voxel, else 0xFFFFFFFF
     bool own_fs = true;              // fs allocated with the buffers (else part of a caller's array)
 };

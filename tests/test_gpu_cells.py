@@ -13,13 +13,14 @@ from helpers import clustered_positions, random_cells, random_field
 pytestmark = pytest.mark.gpu
 
 
-def run_cell_phase(marl, oracle_mod, dims, cells, seed):
+def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32):
     rng = np.random.default_rng(seed)
     X, Y, Z = dims
     f = random_field(dims, rng)
     light = rng.random((Z, Y, X), dtype=np.float32)
     p = marl.default_params()
     ctx = marl.Context(dims, p, cell_capacity=max(len(cells), 1))
+    marl._check(marl.load().marl_ctx_set_cell_lanes(ctx.h, lanes), "marl_ctx_set_cell_lanes")
     ctx.upload_field(f)
     ctx.upload_light(light)
     ctx.upload_cells(cells)
@@ -48,6 +49,26 @@ def test_cell_phase_sparse(marl, oracle_mod, n):
     cells = random_cells(dims, n, np.random.default_rng(n))
     gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, n)
     assert_same(gpu, cpu)
+
+
+@pytest.mark.parametrize("lanes", [1, 5, 8, 16])
+def test_cell_phase_cells_per_warp(marl, oracle_mod, lanes):
+    """Fewer cells per warp ticket (marl_ctx_set_cell_lanes) leave the result
+    unchanged: dense blobs, long dependency chains."""
+    dims = (24, 20, 16)
+    rng = np.random.default_rng(31)
+    pos = clustered_positions(dims, 0.5, rng, 1, 3)
+    cells = random_cells(dims, len(pos), rng, positions=pos)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 78, lanes=lanes)
+    assert_same(gpu, cpu)
+
+
+def test_cell_lanes_rejects_out_of_range(marl):
+    ctx = marl.Context((8, 8, 8), marl.default_params(), cell_capacity=8)
+    lib = marl.load()
+    assert lib.marl_ctx_set_cell_lanes(ctx.h, 0) != 0
+    assert lib.marl_ctx_set_cell_lanes(ctx.h, 33) != 0
+    assert lib.marl_ctx_set_cell_lanes(ctx.h, 32) == 0
 
 
 @pytest.mark.parametrize("frac", [0.05, 0.3, 0.7])
