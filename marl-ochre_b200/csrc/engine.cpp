@@ -213,20 +213,49 @@ bool HostRun::find_empty_neighbor(const uint16_t p[3], uint16_t out[3]) {
     return true;
 }
 
-// crates/marl-sim/src/lib.rs:219-277 (fate processing) -> edit list
+// crates/marl-sim/src/lib.rs:219-277 (fate processing) -> edit list.
+//
+// The reference's order of events and of random draws is kept exactly; what
+// differs is only how the memory is walked.  The cell rows and cell-map
+// entries that the step will touch sit at random places in tens of megabytes,
+// so a first pass over the change list prefetches them all (the misses then
+// overlap instead of following one another), daughters are built in place in
+// the edit list, and the swap_remove bookkeeping keeps an entry per death
+// instead of one per cell.
 marl_status HostRun::process(const marl_change* changes, uint32_t count, EditData& e) {
     tick_div = tick_death = 0;
     e.halve.clear(), e.deaths.clear(), e.move_dst.clear(), e.move_src.clear(), e.births.clear();
-    std::vector<marl_cell> births;
+    const uint32_t n0 = (uint32_t)cells.size();
+    uint32_t n_div = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (changes[k].cell >= n0)
+            return fail(MARL_ERR_STATE, "change list names cell %u of %u", changes[k].cell, n0);
+        n_div += changes[k].event == MARL_EVENT_DIVISION;
+    }
+    // Prefetch: parents' rows and every cell-map entry a placement may probe,
+    // dying cells' rows and voxels.
+    const int dist = (int)sim.division_neighbor_distance;
     for (uint32_t k = 0; k < count; ++k) {
         const marl_change& ch = changes[k];
-        if (ch.cell >= cells.size())
-            return fail(MARL_ERR_STATE, "change list names cell %u of %zu", ch.cell, cells.size());
+        if (ch.event != MARL_EVENT_DIVISION && ch.event != MARL_EVENT_DEATH) continue;
+        const HostCell& c = cells[ch.cell];
+        const char* row = reinterpret_cast<const char*>(&c);
+        for (size_t o = 0; o < sizeof(HostCell); o += 64) __builtin_prefetch(row + o);
+        for (const auto& f : kFace)
+            for (int d : {dist, 1}) {
+                const int nx = c.pos[0] + f[0] * d, ny = c.pos[1] + f[1] * d, nz = c.pos[2] + f[2] * d;
+                if (nx >= 0 && nx < X && ny >= 0 && ny < Y && nz >= 0 && nz < Z) __builtin_prefetch(&cmap[vox(nx, ny, nz)]);
+            }
+    }
+    e.births.reserve(n_div);
+    for (uint32_t k = 0; k < count; ++k) {
+        const marl_change& ch = changes[k];
         if (ch.event == MARL_EVENT_DIVISION) {
             const HostCell& parent = cells[ch.cell];
             uint16_t dpos[3];
             if (find_empty_neighbor(parent.pos, dpos)) {
-                marl_cell d;
+                e.births.emplace_back();
+                marl_cell& d = e.births.back();
                 std::memset(&d, 0, sizeof(d));
                 std::memcpy(d.pos, dpos, sizeof(dpos));
                 d.quiescent = ch.quiescent;
@@ -238,7 +267,6 @@ marl_status HostRun::process(const marl_change* changes, uint32_t count, EditDat
                 d.ruleset = parent.ruleset;
                 e.halve.push_back(ch.cell);
                 marl::fate::mutate_ruleset(d.ruleset, rng, sim);  // cell.rs:406-524
-                births.push_back(d);
                 ++tick_div;
             }
         } else if (ch.event == MARL_EVENT_DEATH) {
@@ -249,39 +277,53 @@ marl_status HostRun::process(const marl_change* changes, uint32_t count, EditDat
     total_div += tick_div;
     total_death += tick_death;
     // Deaths arrive in ascending cell order without duplicates (one event per
-    // cell); remove them back to front with swap_remove, tracking which
-    // original slot ends up in each hole.
-    const uint32_t n0 = (uint32_t)cells.size();
-    std::vector<uint32_t> origin(n0);
-    for (uint32_t i = 0; i < n0; ++i) origin[i] = i;
-    for (auto it = e.deaths.rbegin(); it != e.deaths.rend(); ++it) {
-        const uint32_t i = *it;
+    // cell); remove them back to front with swap_remove.  Only death slots
+    // ever receive another cell, so the original slot of the cell in slot i is
+    // recorded per death (origin_of(i) = i for every other slot).
+    const std::vector<uint32_t>& D = e.deaths;
+    std::vector<uint32_t> org(D.size());
+    std::vector<uint8_t> has(D.size(), 0);
+    auto origin_of = [&](uint32_t i) -> uint32_t {
+        const auto it = std::lower_bound(D.begin(), D.end(), i);
+        if (it == D.end() || *it != i) return i;
+        const size_t k = (size_t)(it - D.begin());
+        return has[k] ? org[k] : i;
+    };
+    for (size_t k = D.size(); k-- > 0;) {
+        const uint32_t i = D[k];
+        const uint32_t last = (uint32_t)cells.size() - 1;
         cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = -1;
-        cells[i] = cells.back();
-        origin[i] = origin[cells.size() - 1];
+        const uint32_t o = origin_of(last);
+        if (i != last) cells[i] = cells[last];
+        org[k] = o;
+        has[k] = 1;
         cells.pop_back();
         if (i < cells.size()) cmap[vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = (int32_t)i;
     }
     e.n_after_deaths = (uint32_t)cells.size();
-    for (uint32_t d : e.deaths)
-        if (d < e.n_after_deaths && origin[d] != d) {
-            e.move_dst.push_back(d);
-            e.move_src.push_back(origin[d]);
+    for (size_t k = 0; k < D.size(); ++k)
+        if (D[k] < e.n_after_deaths && org[k] != D[k]) {
+            e.move_dst.push_back(D[k]);
+            e.move_src.push_back(org[k]);
         }
-    // Births append unless the voxel was taken meanwhile (lib.rs:270-277).
-    for (auto& b : births) {
+    // Births append unless the voxel was taken meanwhile (lib.rs:270-277);
+    // rejected daughters leave the edit list, the others keep their order.
+    size_t w = 0;
+    for (size_t r = 0; r < e.births.size(); ++r) {
+        const marl_cell& b = e.births[r];
         const size_t v = vox(b.pos[0], b.pos[1], b.pos[2]);
-        if (cmap[v] < 0) {
-            cmap[v] = (int32_t)cells.size();
-            HostCell h;
-            std::memcpy(h.pos, b.pos, sizeof(h.pos));
-            h.starter_type = b.starter_type;
-            h.lineage_id = b.lineage_id;
-            h.ruleset = b.ruleset;
-            cells.push_back(h);
-            e.births.push_back(b);
-        }
+        if (cmap[v] >= 0) continue;
+        cmap[v] = (int32_t)cells.size();
+        cells.emplace_back();
+        HostCell& h = cells.back();
+        std::memcpy(h.pos, b.pos, sizeof(h.pos));
+        h.starter_type = b.starter_type;
+        h.lineage_id = b.lineage_id;
+        h.ruleset = b.ruleset;
+        if (w != r) e.births[w] = b;
+        ++w;
     }
+    e.births.resize(w);
     ++tick;
     return MARL_OK;
 }
