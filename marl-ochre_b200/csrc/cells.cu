@@ -379,7 +379,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
         } else {
             active = reactions(c, S);
             if (MODE == kModeGated && spec) {
-                // The plain result is the judge: normwise relative error of the
+                // The plain result decides: normwise relative error of the
                 // prediction, over the 16 species.
                 float num = 0.0f, den = 0.0f;
 #pragma unroll
