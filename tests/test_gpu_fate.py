@@ -96,6 +96,24 @@ def test_fate_step_matches_oracle(marl, oracle_mod, dims, n, probs, seed, tick):
     np.testing.assert_array_equal(gocc, wocc)
 
 
+@pytest.mark.parametrize("dims,n,dist", [
+    ((32, 32, 1), 300, 1),    # one plane: the z faces are off the grid
+    ((20, 20, 20), 2000, 3),  # placement three voxels out
+    ((7, 5, 3), 60, 2),       # ragged grid, more than half occupied
+])
+def test_fate_step_other_geometry(marl, oracle_mod, dims, n, dist):
+    rng = np.random.default_rng(n + dist)
+    cells = mutable_cells(dims, n, rng)
+    events = rng.choice([0, DIV, DEATH, QUIESCENT], size=n, p=(0.4, 0.35, 0.2, 0.05)).astype(np.uint8)
+    p = mutation_params(marl)
+    p.division_neighbor_distance = dist
+    _, gc, gocc, gs = device_step(marl, dims, p, cells, events, 17, 3)
+    _, wc, wocc, ws = oracle_step(oracle_mod, dims, p, cells, events, 17, 3)
+    assert (gs["tick_divisions"], gs["population"]) == (ws["tick_divisions"], ws["population"])
+    assert_same_cells(gc, wc)
+    np.testing.assert_array_equal(gocc, wocc)
+
+
 def test_consecutive_fate_steps(marl, oracle_mod):
     dims = (24, 24, 24)
     rng = np.random.default_rng(5)
