@@ -9,6 +9,7 @@ then the change list to the host, fate/division/mutation on the host, and the
 edit list back.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --case {diffusion,cells,light,mlp,engine} [...]   (one kernel, for ncu)
 
 Printed (rank 0, one JSON line):
   value       ticks/s with all state resident in HBM: K ticks / summed device
@@ -550,6 +551,123 @@ def peaks_bf16() -> float:
         return 1590.0
 
 
+# ----------------------------------------------------------------- cases ----
+# Single-kernel cases on seeded synthetic inputs, for profiling one kernel in
+# isolation (`python bench.py --case ...`).  Each builds a context, uploads the
+# state and runs the kernel a few times; under `ncu -k regex:<kernel> -s <n>
+# -c 1` that captures one launch with the earlier launches as warm-up.  The
+# engine case runs the seed-42 default run: one k_cell_tick launch per tick, so
+# `-k regex:k_cell_tick -s <ticks-1> -c 1` captures the last; with
+# --device-fate all ticks are enqueued at once.
+
+def case_clustered_cells(marl, dims, frac: float, rng: np.random.Generator) -> np.ndarray:
+    """Cells on random balls of radius 2-4 until `frac` of the voxels are covered."""
+    X, Y, Z = dims
+    occ = np.zeros((Z, Y, X), bool)
+    zz, yy, xx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    while occ.sum() < frac * X * Y * Z:
+        r = rng.integers(2, 5)
+        cx, cy, cz = rng.integers(0, X), rng.integers(0, Y), rng.integers(0, Z)
+        occ |= (xx - cx) ** 2 + (yy - cy) ** 2 + (zz - cz) ** 2 <= r * r
+    z, y, x = np.nonzero(occ)
+    c = np.zeros(len(x), marl.CELL_DTYPE)
+    c["pos"] = np.stack([x, y, z], 1)
+    return c
+
+
+def case_random_cells(marl, dims, n: int, rng: np.random.Generator) -> np.ndarray:
+    """n cells with random rulesets at unique random voxels."""
+    X, Y, Z = dims
+    flat = rng.choice(X * Y * Z, size=n, replace=False)
+    z, rem = np.divmod(flat, X * Y)
+    y, x = np.divmod(rem, X)
+    c = np.zeros(n, marl.CELL_DTYPE)
+    c["pos"] = np.stack([x, y, z], 1)
+    c["internal"] = rng.random((n, 16), dtype=np.float32)
+    rx = c["ruleset"]["reactions"]
+    rx["substrate"] = rng.integers(0, 16, (n, 16))
+    rx["product"] = rng.integers(0, 16, (n, 16))
+    rx["catalyst"] = rng.integers(0, 16, (n, 16))
+    rx["cofactor"] = 0xFF
+    rx["k_m"] = (0.01 + 0.99 * rng.random((n, 16))).astype(np.float32)
+    rx["v_max"] = rng.lognormal(0.0, 1.0, (n, 16)).astype(np.float32)
+    rx["k_cat"] = (0.01 + 0.99 * rng.random((n, 16))).astype(np.float32)
+    tp = c["ruleset"]["transport"]
+    tp["uptake_rate"] = rng.random((n, 8), dtype=np.float32)
+    tp["secrete_rate"] = rng.random((n, 8), dtype=np.float32)
+    tp["ext_species"] = rng.integers(0, 12, (n, 8))
+    tp["int_species"] = rng.integers(0, 16, (n, 8))
+    c["ruleset"]["fate"]["division_energy"] = 10.0
+    return c
+
+
+def case_mlp(marl, rows: int, reps: int, rng: np.random.Generator) -> int:
+    """Surrogate inference on `rows` random standardised feature rows, random weights."""
+    import torch
+
+    s = marl.Surrogate(max_pairs=128, batch=128)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)  # inputs are torch tensors
+    params = np.zeros(marl.SURR_PARAMS, np.float32)
+    params[: 256 * 128] = rng.normal(0, 0.1, 256 * 128)
+    params[256 * 128 + 256: 256 * 128 + 256 + 65536] = rng.normal(0, 0.06, 65536)
+    params[-16 - 4096: -16] = rng.normal(0, 0.06, 4096)
+    norm = np.zeros(marl.SURR_NORM, np.float32)
+    norm[93:186] = 1.0
+    norm[202:218] = 1.0
+    s.set_weights(params, norm)
+    x = torch.randn(rows, 128, device="cuda").to(torch.bfloat16)
+    x[:, 93:] = 0
+    y = torch.empty(16, rows, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(reps):
+        s.infer_device(x.data_ptr(), rows, y.data_ptr(), rows)
+    torch.cuda.synchronize()
+    print(f"mlp ok: rows={rows} reps={reps} finite={bool(torch.isfinite(y).all())}")
+    s.close()
+    return 0
+
+
+def run_case(args) -> int:
+    import marl_cuda as marl
+
+    dims = tuple(args.dims)
+    X, Y, Z = dims
+    rng = np.random.default_rng(1)
+    if args.case == "mlp":
+        return case_mlp(marl, args.rows, args.reps, rng)
+    if args.case == "engine":
+        e = marl.Engine(dims, marl.default_params(), rng_seed=42, seed_count=30, cell_capacity=1 << 20)
+        if args.device_fate:
+            e.set_device_fate(True)
+        e.step(args.ticks)
+        print(f"engine ok: dims={dims} ticks={args.ticks} stats={e.stats()}")
+        return 0
+    field = rng.random((Z, Y, X, 12), dtype=np.float32)
+    if args.case == "cells":
+        cells = case_random_cells(marl, dims, args.cells, rng)
+    else:
+        cells = case_clustered_cells(marl, dims, 0.05, rng)
+    ctx = marl.Context(dims, cell_capacity=max(len(cells), 1))
+    ctx.upload_field(field)
+    ctx.upload_cells(cells)
+    if args.case == "diffusion":
+        if args.tile:
+            ctx.set_tile(*args.tile)
+        else:
+            ctx.autotune(3)
+        ctx.diffuse(args.substeps)
+    elif args.case == "cells":
+        ctx.upload_light(rng.random((Z, Y, X), dtype=np.float32))
+        for _ in range(args.reps):
+            ctx.cell_phase()
+    else:
+        for _ in range(args.reps):
+            ctx.light_update()
+    ctx.synchronize()
+    print(f"{args.case} ok: dims={dims} cells={len(cells)} tile={ctx.get_tile()}")
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -558,13 +676,24 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", type=int, nargs=2, metavar=("TILE", "ZC"),
-                    help="fixed diffusion tile index and z-chunk instead of the autotuner (for launch lists)")
+                    help="fixed diffusion tile index and z-chunk instead of the autotuner (launch lists, cases)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the separate diffusion timing")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate leg")
     ap.add_argument("--no-micro", action="store_true", help="skip the field and cell microbenchmarks")
     ap.add_argument("--no-device-fate", action="store_true", help="skip the device-fate engine leg")
+    ap.add_argument("--case", choices=["diffusion", "cells", "light", "mlp", "engine"],
+                    help="instead of the benchmark, run one kernel on seeded synthetic inputs (for ncu)")
+    ap.add_argument("--dims", type=int, nargs=3, default=[128, 128, 64], help="case grid")
+    ap.add_argument("--substeps", type=int, default=8, help="case diffusion: substeps")
+    ap.add_argument("--cells", type=int, default=90, help="case cells: random cells")
+    ap.add_argument("--reps", type=int, default=4, help="case cells/light/mlp: repetitions")
+    ap.add_argument("--rows", type=int, default=300_000, help="case mlp: rows per inference")
+    ap.add_argument("--ticks", type=int, default=1000, help="case engine: ticks of the seed-42 default run")
+    ap.add_argument("--device-fate", action="store_true", help="case engine: fate on the device")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -243,6 +243,22 @@ marl_status marl_ctx_get_tile(marl_ctx* ctx, int32_t* tile, int32_t* zc);
  * per warp serialise less work inside a warp along the dependency chains, at
  * the cost of more warps.  Results do not depend on it. */
 marl_status marl_ctx_set_cell_lanes(marl_ctx* ctx, uint32_t lanes);
+/* Bound of the cell loop's dependency waits (no reference counterpart; the
+ * reference loop is sequential and never waits).  A cell that has polled an
+ * unfinished dependency `polls` times gives up: it is left un-updated with
+ * event None, the phase finishes, and the call that reads the device status
+ * returns MARL_ERR_TIMEOUT.  0 restores the default (4,194,304 polls of at
+ * least 64 ns each). */
+marl_status marl_ctx_set_wait_limit(marl_ctx* ctx, uint32_t polls);
+/* Failure-injection hook for tests (no reference counterpart): during the
+ * next cell phase only, cell `cell` (< population) also waits, through its
+ * face `face` (0..5 in FACE_OFFSETS order, which must be an empty in-grid
+ * voxel), for the completion flag of slot `slot`, with population <= slot <
+ * capacity: a slot that no cell completes in that phase.  The wait runs out
+ * after the limit set by marl_ctx_set_wait_limit and the phase reports
+ * MARL_ERR_TIMEOUT; the phase after it recomputes the true dependencies.  A
+ * face that is occupied or outside the grid gives MARL_ERR_INVALID_INPUT. */
+marl_status marl_ctx_test_hold_dependency(marl_ctx* ctx, uint32_t cell, uint32_t face, uint32_t slot);
 /* Tile autotuner (no reference counterpart): times `reps` substeps of every
  * tile shape / z-chunk candidate on this context's grid with CUDA events and
  * keeps the fastest.  The live field is not modified. */
@@ -318,11 +334,15 @@ marl_status marl_diffuse_device(float* field_dev, float* scratch_dev, const uint
  * word live in one static device array that every GPU loading the library holds
  * until exit (about 13 MiB).  Limits: at most 262,144 voxels, and
  * Y * Z * (X rounded up to 16) <= 1,048,576 bytes of mask; larger grids get
- * MARL_ERR_INVALID_INPUT.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race and
- * must not be issued.  Otherwise identical to marl_diffuse_device (same
- * arguments minus scratch_dev, same results, synchronizes `cuda_stream`). */
+ * MARL_ERR_INVALID_INPUT.  Every call looks up the array's device address
+ * on the current device (cudaGetSymbolAddress, no allocation), so a device
+ * reset by the application does not leave a stale address behind.  The first
+ * call on a device also loads the library's device code, which reserves the
+ * array; it should come before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must not be issued.
+ * Otherwise identical to marl_diffuse_device (same arguments minus
+ * scratch_dev, same results and status codes, MARL_ERR_NO_DEVICE without an
+ * sm_100 device, synchronizes `cuda_stream`). */
 marl_status marl_diffuse_device_noalloc(float* field_dev, const uint8_t* occupancy_dev, int32_t gx, int32_t gy,
                                         int32_t gz, const marl_sim_params* sim, uint32_t substeps,
                                         void* cuda_stream);

@@ -11,6 +11,7 @@ multiply-add contraction) and without fast-math.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -52,7 +53,7 @@ def headers() -> list[str]:
 def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     newest_header = max(os.path.getmtime(h) for h in headers())
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         name = os.path.basename(src)
         obj = os.path.join(BUILD, name + ".o")
@@ -67,7 +68,16 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
+    # Translation units compile independently: run them side by side.
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1) or 1) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=ptxas_v), cmds):
+            if ptxas_v:
+                sys.stdout.write(r.stdout.decode() + r.stderr.decode())
+            if r.returncode != 0:
+                if not ptxas_v:
+                    raise subprocess.CalledProcessError(r.returncode, r.args)
+                raise subprocess.CalledProcessError(r.returncode, r.args, r.stdout, r.stderr)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [nvcc(), "-ccbin", host_cxx(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs]
         if verbose:

@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "kernel_setup.h"
 #include "mlp.h"
 #include "table_ops.cuh"
 
@@ -545,7 +546,7 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
                 }
             }
             if (__any_sync(FULL, pending)) {
-                if (++spins > kFlagSpinLimit) {
+                if (++spins > c.wait_limit) {
                     if (pending) {
                         const CellTable& t = *v.t;
                         atomicOr(err, kErrTimeoutDeps);
@@ -1035,20 +1036,31 @@ cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+__global__ void k_hold_dependency(CellTable t, uint32_t cell, int face, uint32_t slot, uint32_t* err) {
+    if ((t.nb[cell] >> face) & 1u)
+        t.dep[(size_t)face * t.cap + cell] = (int32_t)slot;
+    else
+        atomicOr(err, kErrBadIndex);
+}
+
+cudaError_t launch_hold_dependency(const CellTable& t, uint32_t cell, int face, uint32_t slot, uint32_t* err,
+                                   cudaStream_t s) {
+    k_hold_dependency<<<1, 1, 0, s>>>(t, cell, face, slot, err);
+    return cudaGetLastError();
+}
+
 template <int MODE>
 static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaStream_t s) {
-    static int per_sm = 0, configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_cell_tick<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick<MODE>, kTickThreads, kTickSmem);
-        if (e != cudaSuccess) return e;
-        if (per_sm < 1) per_sm = 1;
-        configured_device = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    int per_sm = 1;
+    cudaError_t e = setup_once(setup, &per_sm, [](int* v) {
+        cudaError_t r = cudaFuncSetAttribute(k_cell_tick<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
+        if (r != cudaSuccess) return r;
+        r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick<MODE>, kTickThreads, kTickSmem);
+        if (*v < 1) *v = 1;
+        return r;
+    });
+    if (e != cudaSuccess) return e;
     const uint32_t warps_needed = (a.n + a.lanes - 1) / a.lanes;
     const uint32_t blocks_needed = (warps_needed + (kTickThreads / 32) - 1) / (kTickThreads / 32);
     // Persistent: never more blocks than can be resident at once, so every
@@ -1073,15 +1085,9 @@ cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
 cudaError_t launch_surrogate_prepass(const CellLaunch& a, const float* norm, float* xt, void* X, int num_sms,
                                      cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_surrogate_prepass, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    cudaError_t e = set_smem_once(setup, k_surrogate_prepass, kTickSmem);
+    if (e != cudaSuccess) return e;
     const uint32_t blocks_needed = (a.n + kTickThreads - 1) / kTickThreads;
     const uint32_t cap_blocks = (uint32_t)num_sms * 8u;
     k_surrogate_prepass<<<blocks_needed < cap_blocks ? blocks_needed : cap_blocks, kTickThreads, kTickSmem, s>>>(
@@ -1093,15 +1099,9 @@ cudaError_t launch_surrogate_prepass_batch(const RunDesc* runs, int n_runs, uint
                                            int parity, const float* norm, float* xt, uint32_t ld, void* X,
                                            int num_sms, cudaStream_t s) {
     if (total == 0) return cudaSuccess;
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_surrogate_prepass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    cudaError_t e = set_smem_once(setup, k_surrogate_prepass_batch, kTickSmem);
+    if (e != cudaSuccess) return e;
     const uint32_t blocks_needed = (total + kTickThreads - 1) / kTickThreads;
     const uint32_t cap_blocks = (uint32_t)num_sms * 8u;
     k_surrogate_prepass_batch<<<blocks_needed < cap_blocks ? blocks_needed : cap_blocks, kTickThreads, kTickSmem, s>>>(
@@ -1176,18 +1176,17 @@ cudaError_t launch_cell_schedule_batch(const RunDesc* runs, int n_runs, int num_
 template <int MODE>
 static cudaError_t launch_cell_tick_batch_mode(const RunDesc* runs, int n_runs, BatchScalars* bs, const CellConsts& k,
                                                int parity, int num_sms, cudaStream_t s) {
-    static int per_sm = 0, configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e =
+    static std::atomic<int> setup[kSetupDevices];
+    int per_sm = 1;
+    cudaError_t e = setup_once(setup, &per_sm, [](int* v) {
+        cudaError_t r =
             cudaFuncSetAttribute(k_cell_tick_batch<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_tick_batch<MODE>, kTickThreads, kTickSmem);
-        if (e != cudaSuccess) return e;
-        if (per_sm < 1) per_sm = 1;
-        configured_device = dev;
-    }
+        if (r != cudaSuccess) return r;
+        r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick_batch<MODE>, kTickThreads, kTickSmem);
+        if (*v < 1) *v = 1;
+        return r;
+    });
+    if (e != cudaSuccess) return e;
     // Persistent over all resident slots; the cell count is read on the device.
     k_cell_tick_batch<MODE><<<per_sm * num_sms, kTickThreads, kTickSmem, s>>>(runs, n_runs, bs, k, parity);
     return cudaGetLastError();

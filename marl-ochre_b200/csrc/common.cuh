@@ -14,7 +14,7 @@ namespace marl {
 // Spin limits.  Every device-side wait is bounded; on expiry the kernel sets a
 // bit in its error word and leaves the wait.
 constexpr uint32_t kMbarSpinLimit = 1u << 22;  // try_wait rounds (each ~ up to a few us)
-constexpr uint32_t kFlagSpinLimit = 1u << 22;  // polls of a dependency flag (with nanosleep)
+constexpr uint32_t kFlagSpinLimit = 1u << 22;  // default polls of a dependency flag (with nanosleep)
 
 // Error bits written by kernels (read back with the change-list header).
 constexpr uint32_t kErrTimeoutMbar = 1u << 0;
@@ -78,6 +78,7 @@ struct CellConsts {
     float dt, c_max, epsilon, thr;
     float lambda_maintenance, reaction_maintenance, hard_death_floor;
     float base_division_prep, prep_maintenance_multiplier, rush_penalty_rate;
+    uint32_t wait_limit;  // polls of a dependency flag before the wait gives up (kErrTimeoutDeps)
 };
 
 struct Grid {

@@ -93,6 +93,7 @@ void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck) {
     ck->base_division_prep = p.base_division_prep;
     ck->prep_maintenance_multiplier = p.prep_maintenance_multiplier;
     ck->rush_penalty_rate = p.rush_penalty_rate;
+    ck->wait_limit = kFlagSpinLimit;
 }
 
 marl_status validate_dims(int32_t gx, int32_t gy, int32_t gz) {
@@ -210,6 +211,7 @@ CellLaunch cell_launch(marl_ctx* c) {
     a.field = c->field[c->cur];
     a.light = c->light;
     a.k = c->ck;
+    a.k.wait_limit = c->wait_limit;
     a.epoch = c->epoch;
     a.ticket = &c->d_hdr->pad[0];
     a.lanes = c->cell_lanes;
@@ -250,6 +252,13 @@ marl_status enqueue_cell_phase(marl_ctx* c) {
         CK(launch_cell_schedule(a, c->stream));
         c->schedule_dirty = false;
         ++c->launches;
+    }
+    if (c->hold_cell >= 0) {  // marl_ctx_test_hold_dependency: this phase only
+        CK(launch_hold_dependency(c->t, (uint32_t)c->hold_cell, c->hold_face, c->hold_slot, &c->d_hdr->err,
+                                  c->stream));
+        ++c->launches;
+        c->hold_cell = -1;
+        c->schedule_dirty = true;  // the next phase recomputes the true dependencies
     }
     c->epoch += 1;
     if (c->epoch == 0) {  // wrapped: clear stale epochs
@@ -526,6 +535,27 @@ marl_status marl_ctx_set_cell_lanes(marl_ctx* c, uint32_t lanes) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
     if (lanes < 1 || lanes > 32) return fail(MARL_ERR_INVALID_INPUT, "lanes %u outside 1..32", lanes);
     c->cell_lanes = lanes;
+    return MARL_OK;
+}
+
+marl_status marl_ctx_set_wait_limit(marl_ctx* c, uint32_t polls) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    c->wait_limit = polls ? polls : kFlagSpinLimit;
+    return MARL_OK;
+}
+
+marl_status marl_ctx_test_hold_dependency(marl_ctx* c, uint32_t cell, uint32_t face, uint32_t slot) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
+    if (cell >= c->n || face >= 6 || slot < c->n || slot >= c->t.cap)
+        return fail(MARL_ERR_INVALID_INPUT, "hold: cell %u (population %u), face %u, slot %u (capacity %u)", cell,
+                    c->n, face, slot, c->t.cap);
+    c->hold_cell = (int32_t)cell;
+    c->hold_face = (int)face;
+    c->hold_slot = slot;
     return MARL_OK;
 }
 

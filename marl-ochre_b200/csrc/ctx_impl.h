@@ -35,6 +35,10 @@ struct marl_ctx {
     bool c4_valid = false;     // c4 equals species 4 of field[cur]
     marl::CellTable t{};
     uint32_t cell_lanes = 32;  // cells per warp ticket of the cell loop
+    uint32_t wait_limit = marl::kFlagSpinLimit;  // polls of a dependency flag (marl_ctx_set_wait_limit)
+    int32_t hold_cell = -1;    // marl_ctx_test_hold_dependency: cell, face and slot for the next phase
+    int hold_face = 0;
+    uint32_t hold_slot = 0;
     uint32_t n = 0;
     uint32_t epoch = 0;
     bool schedule_dirty = true;

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "kernel_setup.h"
 
 namespace marl {
 
@@ -587,15 +588,9 @@ template <int TY, int STAGES>
 static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
                                     int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
     using T = DiffTile<TY, STAGES>;
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(k_diffuse<TY, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             T::SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    cudaError_t e = set_smem_once(setup, k_diffuse<TY, STAGES>, T::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
     dim3 grid((g.X + kDiffTX - 1) / kDiffTX, (g.Y + TY - 1) / TY, (g.Z + plan.zc - 1) / plan.zc);
     k_diffuse<TY, STAGES><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(
         plan.tm_load[which_src], plan.tm_store[which_src ^ 1], plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err);
@@ -622,15 +617,9 @@ static cudaError_t launch_diffuse_batch_t(const RunDesc* runs, const CUtensorMap
                                           uint32_t* err, cudaStream_t s) {
     using T = DiffTile<TY, STAGES>;
     if (n_items == 0) return cudaSuccess;
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(k_diffuse_batch<TY, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             T::SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    cudaError_t e = set_smem_once(setup, k_diffuse_batch<TY, STAGES>, T::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
     k_diffuse_batch<TY, STAGES><<<n_items, kDiffTX * TY, T::SMEM_BYTES, s>>>(runs, maps, items, zc, k, parity,
                                                                            apply_sources, emit_c4, err);
     return cudaGetLastError();

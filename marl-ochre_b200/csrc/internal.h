@@ -153,6 +153,11 @@ struct CellLaunch {
 };
 
 cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s);
+// Test hook: cell `cell` waits through face `face` for slot `slot` (a slot no
+// cell of the tick publishes); kErrBadIndex if that face is not an empty
+// in-grid voxel of the cell (its dependency would not be read).
+cudaError_t launch_hold_dependency(const CellTable& t, uint32_t cell, int face, uint32_t slot, uint32_t* err,
+                                   cudaStream_t s);
 cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s);
 // Surrogate pre-pass: every cell's gather and transport on the current field
 // (as the cell loop would compute them if no earlier cell had written its

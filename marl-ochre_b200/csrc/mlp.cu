@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "kernel_setup.h"
 #include "mlp.h"
 
 namespace marl {
@@ -290,14 +291,9 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(const __grid_constant__ G
 template <int BN, int EPI>
 static cudaError_t launch_one(const GemmArgs& a, int splits, cudaStream_t s) {
     constexpr int smem = 2 * (kBM * 128 + BN * 128) + 1024;
-    static int configured = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured != dev) {
-        cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        configured = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    cudaError_t e = set_smem_once(setup, k_gemm<BN, EPI>, smem);
+    if (e != cudaSuccess) return e;
     dim3 grid((a.M + kBM - 1) / kBM, a.N / BN, splits);
     k_gemm<BN, EPI><<<grid, kGemmThreads, smem, s>>>(a);
     return cudaGetLastError();
@@ -535,14 +531,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(FusedArgs a) {
 
 cudaError_t launch_mlp_fused(const FusedArgs& a, int num_sms, cudaStream_t s) {
     if (a.M <= 0) return cudaSuccess;
-    static int configured = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured != dev) {
-        cudaError_t e = cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem);
-        if (e != cudaSuccess) return e;
-        configured = dev;
-    }
+    static std::atomic<int> setup[kSetupDevices];
+    cudaError_t e = set_smem_once(setup, k_mlp_fused, kFusedSmem);
+    if (e != cudaSuccess) return e;
     const int ntiles = (a.M + kBM - 1) / kBM;
     k_mlp_fused<<<ntiles < num_sms ? ntiles : num_sms, kFusedThreads, kFusedSmem, s>>>(a);
     return cudaGetLastError();

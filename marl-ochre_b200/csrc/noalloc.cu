@@ -17,16 +17,18 @@
 // library holds the array (about 13 MiB) until the process exits.
 //
 // Host code cannot use the array's name as a device address (it is a host-side
-// stand-in).  The first call on each device looks the address up with
-// cudaGetSymbolAddress, with that device current, and caches it; that first
-// call should come before any stream capture.  All calls share the array and
-// it keeps the last call's contents: the mask is rewritten and the error word
-// cleared at the start of every call, and the scratch field is fully written
-// by the first substep before it is read.  Calls that overlap on the GPU (for
-// example on two streams at once) race on the array and must not be issued.
+// stand-in).  Every call looks the address up with cudaGetSymbolAddress, with
+// the caller's device current, before it launches anything: the lookup is
+// cheap and allocates nothing, and a cached address would go stale if the
+// application reset the device (the module, and with it the array, is then
+// loaded again at a new address).  The first call on a device also loads the
+// module, which reserves the array; that first call should come before any
+// stream capture.  All calls share the array and it keeps the last call's
+// contents: the mask is rewritten and the error word cleared at the start of
+// every call, and the scratch field is fully written by the first substep
+// before it is read.  Calls that overlap on the GPU (for example on two
+// streams at once) race on the array and must not be issued.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/marl_cuda.h"
 #include "common.cuh"
@@ -36,6 +38,7 @@ namespace marl {
 marl_status fail(marl_status st, const char* fmt, ...);
 marl_status cuda_fail(cudaError_t e, const char* where);
 void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck);
+marl_status check_device(int* dev, int* sms);
 }  // namespace marl
 
 namespace {
@@ -47,23 +50,12 @@ constexpr size_t kNoAllocBytes = kNoAllocFieldBytes + kNoAllocMaskBytes + 256;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-unsigned char* g_scratch_addr[kMaxDevices] = {};  // device address per device, set up once
-
+// Device address of the scratch array on the current device.
 marl_status scratch_for_current_device(unsigned char** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return marl::cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices) return marl::fail(MARL_ERR_INVALID_INPUT, "device %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return marl::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return marl::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    *out = static_cast<unsigned char*>(p);
     return MARL_OK;
 }
 
@@ -87,9 +79,11 @@ extern "C" marl_status marl_diffuse_device_noalloc(float* field_dev, const uint8
     if (substeps == 0) return MARL_OK;
     if (sim->diffusion_substeps == 0) return fail(MARL_ERR_INVALID_INPUT, "sim.diffusion_substeps == 0");
 
-    unsigned char* base = nullptr;
-    marl_status st = scratch_for_current_device(&base);
+    int dev = 0, sms = 0;
+    marl_status st = check_device(&dev, &sms);  // MARL_ERR_NO_DEVICE without an sm_100 device
     if (st) return st;
+    unsigned char* base = nullptr;
+    if ((st = scratch_for_current_device(&base))) return st;
     float* scratch = reinterpret_cast<float*>(base);
     uint8_t* mask = base + kNoAllocFieldBytes;
     uint32_t* err = reinterpret_cast<uint32_t*>(base + kNoAllocFieldBytes + kNoAllocMaskBytes);

@@ -199,7 +199,8 @@ LIB_PATH = os.path.join(HERE, "libmarl_cuda.so")
 EXPORTED = [
     "marl_sim_params_default", "marl_last_error", "marl_abi_version",
     "marl_ctx_create", "marl_ctx_destroy", "marl_ctx_set_stream", "marl_ctx_set_params", "marl_ctx_synchronize",
-    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_set_cell_lanes", "marl_ctx_autotune", "marl_ctx_counters",
+    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_set_cell_lanes", "marl_ctx_set_wait_limit",
+    "marl_ctx_test_hold_dependency", "marl_ctx_autotune", "marl_ctx_counters",
     "marl_upload_field", "marl_download_field", "marl_upload_light", "marl_download_light",
     "marl_upload_cells", "marl_download_cells", "marl_cell_count", "marl_download_occupancy",
     "marl_apply_boundary_sources", "marl_diffuse", "marl_light_update", "marl_cell_phase", "marl_tick",
@@ -248,6 +249,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_set_tile": (c_int32, [P, c_int32, c_int32]),
         "marl_ctx_get_tile": (c_int32, [P, POINTER(c_int32), POINTER(c_int32)]),
         "marl_ctx_set_cell_lanes": (c_int32, [P, c_uint32]),
+        "marl_ctx_set_wait_limit": (c_int32, [P, c_uint32]),
+        "marl_ctx_test_hold_dependency": (c_int32, [P, c_uint32, c_uint32, c_uint32]),
         "marl_ctx_autotune": (c_int32, [P, c_int32, POINTER(c_float)]),
         "marl_ctx_counters": (c_int32, [P, POINTER(Counters)]),
         "marl_upload_field": (c_int32, [P, P]),
@@ -412,6 +415,16 @@ class Context:
 
     def set_tile(self, tile: int, zc: int) -> None:
         _check(self.lib.marl_ctx_set_tile(self.h, tile, zc), "marl_ctx_set_tile")
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of an unfinished dependency before a cell gives up (0: default)."""
+        _check(self.lib.marl_ctx_set_wait_limit(self.h, polls), "marl_ctx_set_wait_limit")
+
+    def test_hold_dependency(self, cell: int, face: int, slot: int) -> None:
+        """Failure injection for the next cell phase: `cell` also waits, through
+        empty face `face`, for slot `slot` (population <= slot < capacity),
+        which no cell completes; the phase then reports TIMEOUT."""
+        _check(self.lib.marl_ctx_test_hold_dependency(self.h, cell, face, slot), "marl_ctx_test_hold_dependency")
 
     def get_tile(self) -> tuple[int, int]:
         t, z = c_int32(), c_int32()
