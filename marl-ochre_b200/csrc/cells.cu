@@ -323,6 +323,46 @@ __device__ __forceinline__ void surrogate_features(const CellScratch& S, float l
     }
 }
 
+// Maintenance and effectors (phases 3b-4 of CellState::tick, cell.rs:291-329)
+// on the reaction phase's output in S.x; effector secretions go to S.del.
+__device__ __forceinline__ void maintenance_effectors(const CellConsts& c, CellScratch& S, const float4 fate,
+                                                      uint32_t prep, uint32_t quiescent, int active) {
+    const int tid = threadIdx.x;
+    const float dt = c.dt;
+    // Maintenance (cell.rs:291-311)
+    float pm;
+    if (prep > 0) {
+        const float evolved = fmaxf(fate.w, 1.0f);
+        const float rush = fmaxf(c.base_division_prep - evolved, 0.0f);
+        pm = c.prep_maintenance_multiplier + rush * c.rush_penalty_rate;
+    } else {
+        pm = 1.0f;
+    }
+    float x0 = S.x[0][tid];
+    x0 *= 1.0f - c.lambda_maintenance * pm * dt;
+    x0 = fmaxf(x0 - (float)active * c.reaction_maintenance * dt, 0.0f);
+    S.x[0][tid] = x0;
+
+    // Effectors (cell.rs:314-329)
+    if (!quiescent) {
+        const uint4 efi = S.idx[1][tid];
+        const uint32_t efw[4] = {efi.x, efi.y, efi.z, efi.w};
+#pragma unroll
+        for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
+            const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+            const uint32_t k = pair & 0xFF, e = pair >> 8;
+            if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
+            const float2 pr = S.ef[i][tid];
+            const float xk = S.x[k][tid];
+            if (xk > pr.x) {
+                const float amount = div_rn(pr.y * xk, 1.0f + xk) * dt;
+                S.x[k][tid] = fmaxf(xk - amount, 0.0f);
+                S.del[e][tid] = S.del[e][tid] + amount;
+            }
+        }
+    }
+}
+
 // Gather -> tick -> scatter of cell j, after all its dependencies are done.
 // MODE: kModePlain, kModeCapture (also writes the cell's surrogate training
 // row), kModeGated / kModeTrusted (reaction phase from the surrogate where
@@ -340,8 +380,10 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
                               -(long long)g.X * g.Y};
     const int n = __popc(nb);
-    const uint32_t st0 = pre.state;
-    const float dt = c.dt;
+    const uint32_t st = pre.state;
+    uint32_t prep = st & 0xFFFFu;
+    uint32_t quiescent = (st >> 16) & 1u;
+    const float4 fate = S.fate[tid];
 
     // The gathered neighbour values are also the scatter's starting values:
     // no other cell touches N(j) while this cell holds it.
@@ -349,6 +391,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     gather_transport(v, c, S, pre, nv);
 
     int active;
+    bool finished = false;  // maintenance and effectors already applied
     if constexpr (MODE == kModePlain) {
         active = reactions(c, S);
     } else if constexpr (MODE == kModeCapture) {
@@ -380,66 +423,49 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
         } else {
             active = reactions(c, S);
             if (MODE == kModeGated && spec) {
-                // The plain result decides: normwise relative error of the
-                // prediction, over the 16 species.
+                // The plain kernel judges the state the cell keeps: maintenance
+                // and effectors run on the plain reaction output and on the
+                // predicted one, and the prediction is kept only when the two
+                // final states agree within tol (normwise relative error over
+                // the 16 species).  Its effector secretions go with it.
+                float del_t[MARL_S_EXT], xp[MARL_M_INT], dp[MARL_S_EXT];
+#pragma unroll
+                for (int e = 0; e < MARL_S_EXT; ++e) del_t[e] = S.del[e][tid];
+                maintenance_effectors(c, S, fate, prep, quiescent, active);
+#pragma unroll
+                for (int k = 0; k < MARL_M_INT; ++k) {
+                    xp[k] = S.x[k][tid];
+                    S.x[k][tid] = fminf(fmaxf(sv.xt[k * ld + row] + sv.pred[k * ld + row], 0.0f), c.c_max);
+                }
+#pragma unroll
+                for (int e = 0; e < MARL_S_EXT; ++e) {
+                    dp[e] = S.del[e][tid];
+                    S.del[e][tid] = del_t[e];
+                }
+                maintenance_effectors(c, S, fate, prep, quiescent, active);
                 float num = 0.0f, den = 0.0f;
 #pragma unroll
                 for (int k = 0; k < MARL_M_INT; ++k) {
-                    const float xs = fminf(fmaxf(sv.xt[k * ld + row] + sv.pred[k * ld + row], 0.0f), c.c_max);
-                    num = fmaxf(num, fabsf(xs - S.x[k][tid]));
-                    den = fmaxf(den, fabsf(S.x[k][tid]));
+                    num = fmaxf(num, fabsf(S.x[k][tid] - xp[k]));
+                    den = fmaxf(den, fabsf(xp[k]));
                 }
                 err = num / fmaxf(den, 1e-6f);
                 if (err <= sv.tol) {
-#pragma unroll
-                    for (int k = 0; k < MARL_M_INT; ++k)
-                        S.x[k][tid] = fminf(fmaxf(sv.xt[k * ld + row] + sv.pred[k * ld + row], 0.0f), c.c_max);
                     status = kSurrAccepted;
                 } else {
+#pragma unroll
+                    for (int k = 0; k < MARL_M_INT; ++k) S.x[k][tid] = xp[k];
+#pragma unroll
+                    for (int e = 0; e < MARL_S_EXT; ++e) S.del[e][tid] = dp[e];
                     status = kSurrRejected;
                 }
+                finished = true;
             }
         }
         sv.status[row] = status;
         sv.err[row] = err;
     }
-
-    // Maintenance (cell.rs:291-311)
-    const uint32_t st = st0;
-    uint32_t prep = st & 0xFFFFu;
-    uint32_t quiescent = (st >> 16) & 1u;
-    const float4 fate = S.fate[tid];
-    float pm;
-    if (prep > 0) {
-        const float evolved = fmaxf(fate.w, 1.0f);
-        const float rush = fmaxf(c.base_division_prep - evolved, 0.0f);
-        pm = c.prep_maintenance_multiplier + rush * c.rush_penalty_rate;
-    } else {
-        pm = 1.0f;
-    }
-    float x0 = S.x[0][tid];
-    x0 *= 1.0f - c.lambda_maintenance * pm * dt;
-    x0 = fmaxf(x0 - (float)active * c.reaction_maintenance * dt, 0.0f);
-    S.x[0][tid] = x0;
-
-    // Phase 4: effectors (cell.rs:314-329)
-    if (!quiescent) {
-        const uint4 efi = S.idx[1][tid];
-        const uint32_t efw[4] = {efi.x, efi.y, efi.z, efi.w};
-#pragma unroll
-        for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
-            const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
-            const uint32_t k = pair & 0xFF, e = pair >> 8;
-            if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
-            const float2 pr = S.ef[i][tid];
-            const float xk = S.x[k][tid];
-            if (xk > pr.x) {
-                const float amount = div_rn(pr.y * xk, 1.0f + xk) * dt;
-                S.x[k][tid] = fmaxf(xk - amount, 0.0f);
-                S.del[e][tid] = S.del[e][tid] + amount;
-            }
-        }
-    }
+    if (!finished) maintenance_effectors(c, S, fate, prep, quiescent, active);
 
     // Phase 5: fate (cell.rs:332-366)
     const float energy = S.x[0][tid];

@@ -7,6 +7,9 @@
   phase (crates/marl-cell/src/cell.rs:246-285) applied to the captured state.
 - The gated mode at tolerance 0 is the plain tick, bit for bit; counters are
   consistent; the trusted mode runs.
+- Gated at 1e-3 with a network trained in the test, every cell's final state
+  (after maintenance and effectors, cell.rs:291-329) is within 1e-3 of the
+  plain phase's, normwise relative over its 16 species.
 - Training on captured pairs reduces the held-out error, and the trained
   network is within 1e-3 of the plain result on more held-out cells than the
   method without it (no reaction update at all) or the untrained network.
@@ -280,4 +283,41 @@ def test_fused_inference_matches_layerwise_and_oracle(marl, rows):
     print(f"\nrows {rows}: fused vs layerwise {e_layer:.2e}, fused vs oracle {e_ref:.2e}")
     assert e_layer <= 1e-4
     assert e_ref <= 1e-2
+    s.close()
+
+
+def test_gated_final_state_within_tolerance(marl):
+    """A network trained on pairs from a seeded 64x64x32 default run; from a
+    later state of that run one plain and one gated (1e-3) cell phase.  The
+    gate judges the cell's final state, so every cell, accepted or not, ends
+    within 1e-3 of the plain phase (normwise relative, 16 species)."""
+    dims = (64, 64, 32)
+    p = marl.default_params()
+    eng = marl.Engine(dims, p, rng_seed=7, seed_count=30, cell_capacity=1 << 16)
+    s = marl.Surrogate(max_pairs=400_000, batch=4096, lr=2e-3, seed=11)
+    eng.step(20)
+    marl.ctx_set_surrogate(eng.lib.marl_engine_ctx(eng.h), s, marl.SURR_CAPTURE)
+    eng.step(160)
+    marl.ctx_set_surrogate(eng.lib.marl_engine_ctx(eng.h), None, marl.SURR_OFF)
+    s.prepare(s.pair_count())
+    s.train(1500)
+    s.set_lr(5e-4)
+    s.train(1500)
+    eng.step(20)
+    field, cells, light = eng.field(), eng.cells(), eng.light()
+    eng.close()
+    plain = make_ctx(marl, dims, cells, field, light)
+    plain.cell_phase()
+    want = plain.download_cells()["internal"]
+    gated = make_ctx(marl, dims, cells, field, light)
+    marl.ctx_set_surrogate(gated.h, s, marl.SURR_GATED, 1e-3)
+    gated.cell_phase()
+    got = gated.download_cells()["internal"]
+    c = marl.ctx_surrogate_counters(gated.h)
+    err = np.abs(got - want).max(1) / np.maximum(np.abs(want).max(1), 1e-6)
+    print(f"\n{len(cells)} cells: speculated {c['speculated']}, accepted {c['accepted']}, "
+          f"max accepted err {c['max_err']:.3e}, max cell err {err.max():.3e}")
+    assert c["accepted"] > 0
+    assert c["max_err"] <= 1e-3
+    assert err.max() <= 1e-3
     s.close()
