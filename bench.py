@@ -243,6 +243,7 @@ def diffusion_roofline(marl, torch, engine, stream, fixed_tile=None) -> dict:
 
 ENSEMBLE_GRIDS = [(64, 64, 32), (96, 96, 48), (128, 128, 64), (128, 128, 96)]
 MLP_FLOP_PER_CELL = 2 * (93 * 256 + 256 * 256 + 256 * 16)  # algorithmic forward FLOPs (93 inputs)
+TICK_COMPARE = 1000  # the surrogate's tick comparison starts from this tick of the seed-42 run
 
 
 def device_fate_leg(marl, torch, stream, steps: int, warmup: int, flush) -> dict:
@@ -292,50 +293,82 @@ def device_fate_leg(marl, torch, stream, steps: int, warmup: int, flush) -> dict
                     "the host-fate run (same model, different random numbers)"}
 
 
-def ensemble_leg(marl, torch, stream, ticks: int = 30, warmup: int = 3, surrogate=None) -> dict:
-    """Batched ensemble: 64 runs (seeds 0-63), 16 each of four grid sizes, one
-    launch per phase for all runs, graph-captured device tick; with a trained
-    surrogate, the same ticks again in the gated mode at 1e-3."""
+def ensemble_leg(marl, torch, stream, ticks: int = 1000, window: int = 20, surrogate=None) -> dict:
+    """Batched ensemble as configured: 64 runs, seeds 0-63, 16 each of four grid
+    sizes, default seeding, one launch per phase for all runs and a
+    graph-captured device tick, advanced `ticks` ticks from seeding with host
+    fate and timed over all of them (device time and end to end); from the
+    tick-`ticks` state, `window` more plain ticks and then, with a trained
+    surrogate, `window` ticks gated at 1e-3; and the same ensemble with fate on
+    the device, `ticks` ticks from seeding."""
+    runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
 
-    def timed(mode, device_fate=False):
-        runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
-        b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=1 << 16)
+    def make(device_fate):
+        b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=0)
         b.set_stream(stream.cuda_stream)
         us = b.autotune(3)
         if device_fate:
             b.set_device_fate(True)
-        if mode is not None:
-            b.set_surrogate(surrogate, mode, 1e-3)
-        b.step(warmup)
+        return b, us
+
+    def timed(b, n):
         torch.cuda.synchronize()
         c0 = b.counters()
         t0 = time.perf_counter()
-        b.step(ticks)
+        b.step(n)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         c1 = b.counters()
-        dev_s = (c1["device_us"] - c0["device_us"]) / 1e6
-        pop = sum(b.stats(r)["population"] for r in range(len(runs)))
-        out = {"run_ticks_per_s": len(runs) * ticks / dev_s, "e2e_run_ticks_per_s": len(runs) * ticks / wall,
-               "ms_per_batch_tick": 1000.0 * dev_s / ticks, "population_end": int(pop),
-               "autotune_us_per_batched_substep": us}
-        if mode is not None:
-            out["surrogate_counters"] = {k: (float(v) if isinstance(v, float) else int(v))
-                                         for k, v in b.surrogate_counters().items()}
-        b.close()
-        return out
+        return (c1["device_us"] - c0["device_us"]) / 1e6, wall
 
-    res = timed(None)
-    res["workload"] = ("64 runs, seeds 0-63, 16 each of 64x64x32, 96x96x48, 128x128x64, 128x128x96; "
-                       f"ticks {warmup + 1}..{warmup + ticks}")
-    res["note"] = ("device time (CUDA events on the batch stream) of the graph-replayed device ticks and edit "
+    def population(b):
+        return int(sum(b.stats(r)["population"] for r in range(len(runs))))
+
+    def whole_run(b, us):
+        dev = wall = 0.0
+        trajectory = []
+        chunk = max(ticks // 10, 1)
+        done = 0
+        while done < ticks:
+            n = min(chunk, ticks - done)
+            d, w = timed(b, n)
+            dev += d
+            wall += w
+            done += n
+            trajectory.append({"tick": done, "population": population(b),
+                               "run_ticks_per_s": len(runs) * n / d})
+        return {"ticks": f"1..{ticks}", "run_ticks_per_s": len(runs) * ticks / dev,
+                "e2e_run_ticks_per_s": len(runs) * ticks / wall, "ms_per_batch_tick": 1000.0 * dev / ticks,
+                "population_end": population(b), "population_trajectory": trajectory,
+                "autotune_us_per_batched_substep": us}
+
+    b, us = make(False)
+    res = whole_run(b, us)
+    res["workload"] = ("64 runs, seeds 0-63, 16 each of 64x64x32, 96x96x48, 128x128x64, 128x128x96, default "
+                       f"seeding; ticks 1..{ticks} from seeding, host fate")
+    res["note"] = ("device time: CUDA events on the batch stream around the graph-replayed device ticks and edit "
                    "copies; e2e adds the host fate step of all runs on worker threads")
+    d, w = timed(b, window)
+    res["plain_window"] = {"ticks": f"{ticks + 1}..{ticks + window}", "run_ticks_per_s": len(runs) * window / d,
+                           "e2e_run_ticks_per_s": len(runs) * window / w, "population_end": population(b)}
     if surrogate is not None:
-        res["with_surrogate_gated_1e-3"] = timed(marl.SURR_GATED)
-    res["with_device_fate"] = timed(None, device_fate=True)
+        b.set_surrogate(surrogate, marl.SURR_GATED, 1e-3)
+        d, w = timed(b, window)
+        cnt = b.surrogate_counters()
+        res["gated_1e-3_window"] = {
+            "ticks": f"{ticks + window + 1}..{ticks + 2 * window}", "run_ticks_per_s": len(runs) * window / d,
+            "e2e_run_ticks_per_s": len(runs) * window / w, "population_end": population(b),
+            "surrogate_counters": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in cnt.items()},
+            "note": "max_err: largest normwise error, over the 16 species, of an accepted cell's final state "
+                    "(after maintenance and effectors) against the plain kernel's"}
+        b.set_surrogate(None, marl.SURR_OFF)
+    b.close()
+    bd, us = make(True)
+    res["with_device_fate"] = whole_run(bd, us)
     res["with_device_fate"]["note"] = ("fate of every run on the device: one CUDA graph per batch tick, one "
                                        "synchronisation per step call; per-division random streams, so the "
                                        "trajectories differ from the host-fate runs")
+    bd.close()
     return res
 
 
@@ -401,10 +434,11 @@ def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int
     infer_s = ev0.elapsed_time(ev1) / 1000.0 / reps
     tflops = MLP_FLOP_PER_CELL * n_cells / infer_s / 1e12
 
-    # The tick in each mode, from one state of a long default run.
+    # The tick in each mode, from the tick-1000 state of the seed-42 default run
+    # (the run's population at the end of the configured 1000 ticks).
     e = marl.Engine(DIMS, p, rng_seed=SEED, seed_count=SEED_COUNT, cell_capacity=1 << 20)
     e.set_stream(stream.cuda_stream)
-    e.step(400)
+    e.step(TICK_COMPARE)
     field, cells, light = e.field(), e.cells(), e.light()
     e.close()
     modes = {}
@@ -444,8 +478,11 @@ def surrogate_leg(marl, torch, stream, budget_s: float = 45.0, target_pairs: int
         modes[name]["cell_phase_cells_within_1e-3"] = float((err <= 1e-3).mean())
     return s, {
         "workload": f"pairs from {seed - 100} seeded 128x128x64 default runs (ticks 21..<=600), "
-                    f"{n} rows, last 5% held out; tick comparison from tick 400 of the seed-{SEED} run "
-                    f"({len(cells)} cells)",
+                    f"{n} rows, last 5% held out; tick comparison from tick {TICK_COMPARE} of the seed-{SEED} "
+                    f"run ({len(cells)} cells)",
+        "population_note": "the configured ~300k cells at 128x128x64 are not reached by the seeded default run: it "
+                           "holds 38k cells at tick 1000 and 57k at tick 1600 (29% occupancy would be 300k); the "
+                           "300k-row figure is the inference leg's, on synthetic rows",
         "pairs": n, "capture_s": t_cap, "train_steps": steps, "train_batch": 8192, "train_s": t_train,
         "train_lr_schedule": "2e-3 x 16000, 5e-4 x 16000, 1e-4 x 8000 steps",
         "loss_first": float(losses[0][:20].mean()), "loss_last": float(losses[-1][-100:].mean()),
@@ -679,6 +716,7 @@ def main() -> int:
                     help="fixed diffusion tile index and z-chunk instead of the autotuner (launch lists, cases)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the separate diffusion timing")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--ensemble-ticks", type=int, default=1000, help="ticks of the 64-run ensemble from seeding")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate leg")
     ap.add_argument("--no-micro", action="store_true", help="skip the field and cell microbenchmarks")
     ap.add_argument("--no-device-fate", action="store_true", help="skip the device-fate engine leg")
@@ -770,7 +808,7 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_surrogate:
         trained, surr = surrogate_leg(marl, torch, stream)
     if rank == 0 and world == 1 and not args.no_ensemble:
-        ens = ensemble_leg(marl, torch, stream, surrogate=trained)
+        ens = ensemble_leg(marl, torch, stream, ticks=args.ensemble_ticks, surrogate=trained)
     if trained is not None:
         trained.close()
     if rank == 0:

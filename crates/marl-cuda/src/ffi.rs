@@ -234,6 +234,7 @@ pub struct Stats {
     pub bottom: u64,
     pub avg_energy: f64,
     pub avg_enzyme: f64,
+    pub avg_enzyme_b: f64,
     pub avg_active_reactions: f64,
     pub oxidant_top: f32,
     pub oxidant_middle: f32,

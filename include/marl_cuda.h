@@ -403,7 +403,8 @@ typedef struct marl_stats {
     uint64_t population;
     uint64_t top, middle, bottom;   /* cells with z < Z/3, < 2(Z/3), the rest */
     double avg_energy;              /* mean internal[0] */
-    double avg_enzyme;              /* mean internal[5] */
+    double avg_enzyme;              /* mean internal[5] (ticks.csv avg_enzyme_a) */
+    double avg_enzyme_b;            /* mean internal[6] (ticks.csv avg_enzyme_b, data.rs:214-217) */
     double avg_active_reactions;    /* mean count of reactions with |v_max| > 1e-9 */
     float oxidant_top;              /* field at (X/2, Y/2, 0), species 1 */
     float oxidant_middle;           /* (X/2, Y/2, Z/2), species 1 */

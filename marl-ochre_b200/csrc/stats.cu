@@ -4,10 +4,12 @@
 // and the field.
 //
 // Counts (population, per-z-third, per-z) and the centre-column samples are
-// exact.  The reference averages internal species 0 and 5 and the active
-// reaction count with sequential f32 sums (stats.rs:22-34); here the sums are
-// FP64 (per-thread partials, warp shuffles, one FP64 atomic per block), which
-// is the exact average up to FP64 rounding rather than the f32 sum's.
+// exact.  The averages of internal species 0, 5 and 6 and of the active
+// reaction count are the ticks.csv columns of DataLogger::log_tick, which the
+// reference accumulates in f64 (crates/marl-output/src/data.rs:207-232); they
+// are summed in FP64 here too (per-thread partials, warp shuffles, one FP64
+// atomic per block).  print_stats averages the same quantities with f32 sums
+// (stats.rs:22-34); the FP64 result is the exact average up to FP64 rounding.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -25,6 +27,7 @@ constexpr int kStatsMaxZ = 1024;
 struct StatsAccum {
     double energy_sum;
     double enzyme_sum;
+    double enzyme_b_sum;
     double active_sum;
     unsigned long long thirds[3];
     unsigned long long per_z[kStatsMaxZ];
@@ -39,10 +42,11 @@ __global__ void __launch_bounds__(kStatsThreads) k_cell_stats(CellTable t, uint3
     if (threadIdx.x < 3) s_third[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t z_third = (uint32_t)(Z / 3);
-    double e = 0.0, enz = 0.0, act = 0.0;
+    double e = 0.0, enz = 0.0, enzb = 0.0, act = 0.0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         e += (double)t.internal[j];                 // internal[0]
         enz += (double)t.internal[5 * (size_t)t.cap + j];
+        enzb += (double)t.internal[6 * (size_t)t.cap + j];
         int a = 0;
 #pragma unroll
         for (int r = 0; r < MARL_R_MAX; ++r) a += fabsf(__uint_as_float(t.rx[(size_t)r * t.cap + j].z)) > thr ? 1 : 0;
@@ -55,11 +59,13 @@ __global__ void __launch_bounds__(kStatsThreads) k_cell_stats(CellTable t, uint3
     for (int o = 16; o > 0; o >>= 1) {
         e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
         enz += __shfl_xor_sync(0xFFFFFFFFu, enz, o);
+        enzb += __shfl_xor_sync(0xFFFFFFFFu, enzb, o);
         act += __shfl_xor_sync(0xFFFFFFFFu, act, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&acc->energy_sum, e);
         atomicAdd(&acc->enzyme_sum, enz);
+        atomicAdd(&acc->enzyme_b_sum, enzb);
         atomicAdd(&acc->active_sum, act);
     }
     __syncthreads();
@@ -126,6 +132,7 @@ marl_status marl_ctx_stats(marl_ctx* c, marl_stats* out, uint32_t* cells_per_z, 
     if (c->n) {
         out->avg_energy = h.energy_sum / c->n;
         out->avg_enzyme = h.enzyme_sum / c->n;
+        out->avg_enzyme_b = h.enzyme_b_sum / c->n;
         out->avg_active_reactions = h.active_sum / c->n;
     }
     const int zm = g.Z / 2;

@@ -150,6 +150,7 @@ class SurrogateCounters(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("population", c_uint64), ("top", c_uint64), ("middle", c_uint64), ("bottom", c_uint64),
                 ("avg_energy", ctypes.c_double), ("avg_enzyme", ctypes.c_double),
+                ("avg_enzyme_b", ctypes.c_double),
                 ("avg_active_reactions", ctypes.c_double), ("oxidant_top", c_float), ("oxidant_middle", c_float),
                 ("reductant_bottom", c_float), ("organic_middle", c_float)]
 

@@ -19,6 +19,7 @@ def host_stats(cells, field, light, dims):
         "top": int((z < zt).sum()), "middle": int(((z >= zt) & (z < 2 * zt)).sum()), "bottom": int((z >= 2 * zt).sum()),
         "avg_energy": cells["internal"][:, 0].astype(np.float64).sum() / n,
         "avg_enzyme": cells["internal"][:, 5].astype(np.float64).sum() / n,
+        "avg_enzyme_b": cells["internal"][:, 6].astype(np.float64).sum() / n,
         "avg_active_reactions": (np.abs(vmax) > np.float32(1e-9)).sum() / n,
         "oxidant_top": field[0, Y // 2, X // 2, 1], "oxidant_middle": field[Z // 2, Y // 2, X // 2, 1],
         "reductant_bottom": field[Z - 1, Y // 2, X // 2, 2], "organic_middle": field[Z // 2, Y // 2, X // 2, 4],
@@ -36,7 +37,7 @@ def test_device_stats_match_host(marl, dims, ticks):
     assert got["population"] == want["population"] > 0
     for k in ("top", "middle", "bottom"):
         assert got[k] == want[k], k
-    for k in ("avg_energy", "avg_enzyme", "avg_active_reactions"):
+    for k in ("avg_energy", "avg_enzyme", "avg_enzyme_b", "avg_active_reactions"):
         assert got[k] == pytest.approx(want[k], rel=1e-12, abs=1e-15), k
     for k in ("oxidant_top", "oxidant_middle", "reductant_bottom", "organic_middle"):
         assert np.float32(got[k]) == np.float32(want[k]), k
