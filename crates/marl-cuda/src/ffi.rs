@@ -36,6 +36,10 @@ pub const MARL_EVENT_QUIESCENCE: u8 = 3;
 pub const MARL_SOURCES_ADDITIVE: u32 = 0;
 pub const MARL_SOURCES_DIRICHLET: u32 = 1;
 
+pub const MARL_RULESETS_LAYERS: i32 = 1;
+pub const MARL_RULESETS_FULL: i32 = 2;
+pub const MARL_RULESETS_BOTH: i32 = 3;
+
 pub const MARL_SURR_FEATURES: usize = 93;
 pub const MARL_SURR_RAW_STRIDE: usize = 112;
 pub const MARL_SURR_PARAMS: usize = 256 * 128 + 256 + 256 * 256 + 256 + 16 * 256 + 16;
@@ -373,6 +377,9 @@ unsafe extern "C" {
     pub fn marl_ctx_viewer_cells(ctx: *mut Ctx, out: *mut u8, cap_bytes: u64, n_out: *mut u32) -> Status;
     pub fn marl_write_dump(dir: *const c_char, tick: u64, gx: i32, gy: i32, gz: i32, field: *const f32,
                            viewer_cells: *const u8, n_cells: u32) -> Status;
+    pub fn marl_ctx_write_ruleset_dumps(ctx: *mut Ctx, dir: *const c_char, tick: u64, mode: i32) -> Status;
+    pub fn marl_write_ruleset_dumps(dir: *const c_char, tick: u64, gx: i32, gy: i32, gz: i32, cells: *const Cell,
+                                    n: u32, mode: i32) -> Status;
     pub fn marl_ruleset_pack_canonical(rs: *const Ruleset, out: *mut u8) -> Status;
     pub fn marl_ruleset_unpack_canonical(input: *const u8, rs: *mut Ruleset) -> Status;
 

@@ -432,6 +432,30 @@ marl_status marl_ctx_viewer_cells(marl_ctx* ctx, uint8_t* out, uint64_t cap_byte
 marl_status marl_write_dump(const char* dir, uint64_t tick, int32_t gx, int32_t gy, int32_t gz, const float* field,
                             const uint8_t* viewer_cells, uint32_t n_cells);
 
+/* Ruleset sidecar dumps (crates/marl-output/src/binary_dump.rs:121-350,
+ * formats crates/marl-format/src/lib.rs:51-98), uncompressed:
+ *   MARL_RULESETS_LAYERS: <dir>/tick_<tick>.ruleset_layers.bin, one 448-byte
+ *     record per z layer (z u16, 0 u16, cell count u32, then the averages of
+ *     the 110 float fields of the rulesets of the layer's cells: receptors,
+ *     transporter rates, reaction k_m/v_max/k_cat, effector threshold/rate,
+ *     fate, hgt_propensity, mutation_rate), summed in f64 in cell-vector
+ *     order and rounded to f32, as the reference does;
+ *   MARL_RULESETS_FULL: <dir>/tick_<tick>.rulesets.bin, the "MRSF" version-1
+ *     deduplicated dump: a 24-byte header, the distinct canonical 536-byte
+ *     rulesets in order of first occurrence, then per cell (x, y, z) u16 and
+ *     its dictionary id u32.
+ * Each call also rewrites <dir>/run_meta.json with ruleset_output_mode and
+ * the sidecar layout keys (the keys marl_write_dump writes plus the ruleset
+ * ones), so call it after marl_write_dump for the same directory.
+ * marl_ctx_write_ruleset_dumps reduces the layer averages on the device
+ * (Z x 448 bytes cross to the host) and packs the canonical rulesets on the
+ * device (deduplicated on the host); marl_write_ruleset_dumps does the same
+ * from host cells.  The two give identical files. */
+enum { MARL_RULESETS_LAYERS = 1, MARL_RULESETS_FULL = 2, MARL_RULESETS_BOTH = 3 };
+marl_status marl_ctx_write_ruleset_dumps(marl_ctx* ctx, const char* dir, uint64_t tick, int32_t mode);
+marl_status marl_write_ruleset_dumps(const char* dir, uint64_t tick, int32_t gx, int32_t gy, int32_t gz,
+                                     const marl_cell* cells, uint32_t n, int32_t mode);
+
 /* ---- formats ------------------------------------------------------------ */
 /* Canonical 536-byte ruleset payload (crates/marl-format/src/lib.rs:70-89). */
 marl_status marl_ruleset_pack_canonical(const marl_ruleset* rs, uint8_t out[536]);

@@ -187,6 +187,23 @@ def write_dump(directory: str, tick: int, dims, field: np.ndarray | None, cells:
                                0 if c is None else c.size), "marl_write_dump")
 
 
+RULESETS_LAYERS, RULESETS_FULL, RULESETS_BOTH = 1, 2, 3
+
+
+def ctx_write_ruleset_dumps(ctx_handle, directory: str, tick: int, mode: int = RULESETS_BOTH) -> None:
+    """marl_ctx_write_ruleset_dumps: ruleset sidecars of a context's cells (device reductions)."""
+    _check(load().marl_ctx_write_ruleset_dumps(ctx_handle, os.fsencode(directory), tick, mode),
+           "marl_ctx_write_ruleset_dumps")
+
+
+def write_ruleset_dumps(directory: str, tick: int, dims, cells: np.ndarray, mode: int = RULESETS_BOTH) -> None:
+    """marl_write_ruleset_dumps: the same sidecars from host cells (CELL_DTYPE records)."""
+    X, Y, Z = dims
+    c = np.ascontiguousarray(cells, CELL_DTYPE)
+    _check(load().marl_write_ruleset_dumps(os.fsencode(directory), tick, X, Y, Z, _ptr(c) if c.size else None,
+                                           c.size, mode), "marl_write_ruleset_dumps")
+
+
 SURR_FEATURES = 93
 SURR_RAW_STRIDE = 112
 SURR_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 16 * 256 + 16
@@ -221,7 +238,8 @@ EXPORTED = [
     "marl_surrogate_get_weights", "marl_surrogate_set_weights", "marl_surrogate_gradients",
     "marl_surrogate_infer_device", "marl_ctx_set_surrogate", "marl_ctx_surrogate_counters",
     "marl_batch_set_surrogate", "marl_batch_surrogate_counters", "marl_surrogate_set_inference",
-    "marl_ctx_stats", "marl_ctx_viewer_cells", "marl_write_dump",
+    "marl_ctx_stats", "marl_ctx_viewer_cells", "marl_write_dump", "marl_ctx_write_ruleset_dumps",
+    "marl_write_ruleset_dumps",
     "marl_ctx_fate_init", "marl_ctx_fate", "marl_ctx_fate_stats", "marl_ctx_set_events", "marl_ctx_run_ticks",
     "marl_fate_stream_probe", "marl_fate_stream_ln", "marl_engine_set_device_fate", "marl_batch_set_device_fate",
 ]
@@ -324,6 +342,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_stats": (c_int32, [P, POINTER(Stats), P, P]),
         "marl_ctx_viewer_cells": (c_int32, [P, P, c_uint64, POINTER(c_uint32)]),
         "marl_write_dump": (c_int32, [c_char_p, c_uint64, c_int32, c_int32, c_int32, P, P, c_uint32]),
+        "marl_ctx_write_ruleset_dumps": (c_int32, [P, c_char_p, c_uint64, c_int32]),
+        "marl_write_ruleset_dumps": (c_int32, [c_char_p, c_uint64, c_int32, c_int32, c_int32, P, c_uint32, c_int32]),
         "marl_ctx_fate_init": (c_int32, [P, c_uint64, c_uint64, c_uint64, c_uint64]),
         "marl_ctx_fate": (c_int32, [P]),
         "marl_ctx_fate_stats": (c_int32, [P, POINTER(FateStats)]),
