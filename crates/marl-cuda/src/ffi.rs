@@ -332,6 +332,11 @@ unsafe extern "C" {
     pub fn marl_ctx_set_cell_lanes(ctx: *mut Ctx, lanes: u32) -> Status;
     pub fn marl_ctx_set_wait_limit(ctx: *mut Ctx, polls: u32) -> Status;
     pub fn marl_ctx_test_hold_dependency(ctx: *mut Ctx, cell: u32, face: u32, slot: u32) -> Status;
+    pub fn marl_ctx_set_receptor_output(ctx: *mut Ctx, enable: i32) -> Status;
+    pub fn marl_ctx_download_receptor_activations(ctx: *mut Ctx, out: *mut f32, cap_cells: u32, n_out: *mut u32)
+        -> Status;
+    pub fn marl_ctx_hgt(ctx: *mut Ctx, donors: *const u32, recipients: *const u32, n_pairs: u32, seed: u64,
+                        tick: u64) -> Status;
     pub fn marl_ctx_autotune(ctx: *mut Ctx, reps: i32, best_us_per_substep: *mut f32) -> Status;
     pub fn marl_ctx_counters(ctx: *mut Ctx, out: *mut Counters) -> Status;
     pub fn marl_upload_field(ctx: *mut Ctx, field: *const f32) -> Status;

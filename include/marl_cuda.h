@@ -259,6 +259,28 @@ marl_status marl_ctx_set_wait_limit(marl_ctx* ctx, uint32_t polls);
  * MARL_ERR_TIMEOUT; the phase after it recomputes the true dependencies.  A
  * face that is occupied or outside the grid gives MARL_ERR_INVALID_INPUT. */
 marl_status marl_ctx_test_hold_dependency(marl_ctx* ctx, uint32_t cell, uint32_t face, uint32_t slot);
+/* Receptor pass (phase 1 of CellState::tick, crates/marl-cell/src/cell.rs:
+ * 206-220) as an optional output.  The reference computes each receptor's
+ * Hill activation gain * c^n / (k^n + c^n + 1e-9) from the environment the
+ * cell gathered and keeps it in an unused local (receptor-gated transport is
+ * not wired upstream, cell.rs:203-205).  With the output on, every cell phase
+ * writes each updated cell's 8 activations; they change nothing else.
+ * marl_ctx_download_receptor_activations copies the last phase's [n][8]
+ * activations (MARL_ERR_STATE when the output is off; powf as CUDA computes
+ * it, within 1e-5 relative of the reference's). */
+marl_status marl_ctx_set_receptor_output(marl_ctx* ctx, int32_t enable);
+marl_status marl_ctx_download_receptor_activations(marl_ctx* ctx, float* out, uint32_t cap_cells, uint32_t* n_out);
+/* Horizontal gene transfer (crates/marl-cell/src/hgt.rs:7-27,
+ * transfer_reaction; defined upstream, not called by its tick loop) for the
+ * pairs (donors[k], recipients[k]), k = 0..n_pairs-1, in that order: a
+ * random active reaction (|v_max| > 1e-9) of the donor overwrites the
+ * recipient's first inactive slot, or a random slot when all are active.
+ * Pair k draws from its own counter-based stream keyed by (seed, tick, k)
+ * (the device fate stream specification), so results do not depend on
+ * scheduling; independent pairs run in parallel.  Indices are cell indices
+ * (< population). */
+marl_status marl_ctx_hgt(marl_ctx* ctx, const uint32_t* donors, const uint32_t* recipients, uint32_t n_pairs,
+                         uint64_t seed, uint64_t tick);
 /* Tile autotuner (no reference counterpart): times `reps` substeps of every
  * tile shape / z-chunk candidate on this context's grid with CUDA events and
  * keeps the fastest.  The live field is not modified. */

@@ -149,6 +149,7 @@ struct CellRunView {
     const float* light;
     uint32_t epoch;
     const SurrView* sv;  // surrogate modes only
+    float* act;          // receptor activations [8][cap], or null
 };
 
 __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j, CellPre& pre) {
@@ -254,6 +255,29 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
         S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
     }
     S.x[MARL_M_INT - 1][tid] = light;  // cell.rs:243
+}
+
+// Phase 1 of CellState::tick (cell.rs:206-220): receptor i's Hill activation
+// from gathered species i, into act[i][j].  The reference computes it into an
+// unused local; here it is an optional output.  Not inlined, so that the
+// update's register allocation does not carry it when the output is off.
+__device__ __noinline__ void receptor_activations(const CellConsts& c, const CellTable& t, uint32_t j,
+                                                  const CellScratch& S, float* act) {
+    const float* r = t.cold + (size_t)j * kColdFloats;  // receptors: k_half, n_hill, gain
+#pragma unroll 1
+    for (int i = 0; i < MARL_S_RECEPTORS; ++i) {
+        float a = 0.0f;
+        const float gain = r[3 * i + 2];
+        if (fabsf(gain) > c.thr) {
+            const float cc = S.ext[i][threadIdx.x];
+            const float k = fmaxf(r[3 * i], 1e-6f);
+            const float n = rclamp(r[3 * i + 1], c.hill_lo, c.hill_hi);
+            const float kn = powf(k, n);
+            const float cn = powf(fmaxf(cc, 0.0f), n);
+            a = div_rn(gain * cn, kn + cn + 1e-9f);
+        }
+        act[(size_t)i * t.cap + j] = a;
+    }
 }
 
 // Phase 3 of CellState::tick: the reactions, strictly in slot order
@@ -389,6 +413,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     // no other cell touches N(j) while this cell holds it.
     float4 nv[6][3];
     gather_transport(v, c, S, pre, nv);
+    if (v.act) receptor_activations(c, t, j, S, v.act);
 
     int active;
     bool finished = false;  // maintenance and effectors already applied
@@ -595,7 +620,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constan
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const uint32_t total = a.n_dev ? *a.n_dev : a.n;
     cell_tick_loop<MODE>(S, a.k, total, a.ticket, a.err, a.lanes, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
-        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv};
+        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv, a.act};
         j = gi;
     });
 }
@@ -639,7 +664,7 @@ __global__ void __launch_bounds__(kTickThreads) k_surrogate_prepass(const __grid
                                                                    __nv_bfloat16* __restrict__ X) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    const CellRunView v{&a.t, a.g, a.field, a.light, a.epoch, nullptr};
+    const CellRunView v{&a.t, a.g, a.field, a.light, a.epoch, nullptr, nullptr};
     for (uint32_t base = blockIdx.x * kTickThreads; base < a.n; base += gridDim.x * kTickThreads) {
         const uint32_t j = base + threadIdx.x;
         if (j < a.n) prepass_cell(v, a.k, S, j, j, a.t.cap, norm, xt, X);
@@ -658,7 +683,7 @@ __global__ void __launch_bounds__(kTickThreads) k_surrogate_prepass_batch(const 
         const uint32_t gi = base + threadIdx.x;
         if (gi < total) {
             const RunDesc& R = runs[find_run(runs, n_runs, gi)];
-            const CellRunView v{&R.t, R.g, R.field[parity], R.light, R.epoch, nullptr};
+            const CellRunView v{&R.t, R.g, R.field[parity], R.light, R.epoch, nullptr, nullptr};
             prepass_cell(v, c, S, gi - R.cell_base, gi, ld, norm, xt, X);
         }
     }
@@ -705,7 +730,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc*
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     cell_tick_loop<MODE>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, 32u, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         const RunDesc& R = runs[find_run(runs, n_runs, gi)];
-        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv};
+        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv, nullptr};
         j = gi - R.cell_base;
     });
 }

@@ -79,6 +79,7 @@ struct CellConsts {
     float lambda_maintenance, reaction_maintenance, hard_death_floor;
     float base_division_prep, prep_maintenance_multiplier, rush_penalty_rate;
     uint32_t wait_limit;  // polls of a dependency flag before the wait gives up (kErrTimeoutDeps)
+    float hill_lo, hill_hi;  // receptor Hill exponent clamp (receptor activations)
 };
 
 struct Grid {

@@ -94,6 +94,8 @@ void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck) {
     ck->prep_maintenance_multiplier = p.prep_maintenance_multiplier;
     ck->rush_penalty_rate = p.rush_penalty_rate;
     ck->wait_limit = kFlagSpinLimit;
+    ck->hill_lo = p.hill_exponent_clamp_low;
+    ck->hill_hi = p.hill_exponent_clamp_high;
 }
 
 marl_status validate_dims(int32_t gx, int32_t gy, int32_t gz) {
@@ -149,7 +151,7 @@ void ctx_free(marl_ctx* c) {
     void* dev[] = {c->field[0], c->field[1], c->mask, c->cmap, c->light, c->c4, c->d_hdr, c->d_changes, c->d_block_counts,
                    c->d_edit, c->d_mass_partial, c->d_mass_out, c->d_records, c->d_occ_stage, c->d_seam_mask,
                    c->d_events_stage, c->surr_xt, c->surr_pred, c->surr_x, c->surr_status, c->surr_err,
-                   c->surr_counters};
+                   c->surr_counters, c->receptor_act};
     for (void* p : dev)
         if (p) cudaFree(p);
     void* host[] = {c->h_hdr, c->h_edit, c->h_records, c->h_mass};
@@ -216,6 +218,7 @@ CellLaunch cell_launch(marl_ctx* c) {
     a.ticket = &c->d_hdr->pad[0];
     a.lanes = c->cell_lanes;
     a.err = &c->d_hdr->err;
+    a.act = c->receptor_act;
     return a;
 }
 
@@ -556,6 +559,41 @@ marl_status marl_ctx_test_hold_dependency(marl_ctx* c, uint32_t cell, uint32_t f
     c->hold_cell = (int32_t)cell;
     c->hold_face = (int)face;
     c->hold_slot = slot;
+    return MARL_OK;
+}
+
+marl_status marl_ctx_set_receptor_output(marl_ctx* c, int32_t enable) {
+    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
+    if (enable && !c->receptor_act) {
+        CK(cudaMalloc((void**)&c->receptor_act, (size_t)MARL_S_RECEPTORS * c->t.cap * sizeof(float)));
+        CK(cudaMemsetAsync(c->receptor_act, 0, (size_t)MARL_S_RECEPTORS * c->t.cap * sizeof(float), c->stream));
+    } else if (!enable && c->receptor_act) {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(c->receptor_act);
+        c->receptor_act = nullptr;
+    }
+    return MARL_OK;
+}
+
+marl_status marl_ctx_download_receptor_activations(marl_ctx* c, float* out, uint32_t cap, uint32_t* n_out) {
+    if (!c || !n_out || (cap && !out)) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    if (!c->receptor_act) return fail(MARL_ERR_STATE, "receptor output is off (marl_ctx_set_receptor_output)");
+    if (c->n_on_device) {
+        marl_status sp = sync_population(c);
+        if (sp) return sp;
+    }
+    const uint32_t n = c->n;
+    *n_out = n;
+    if (n > cap) return fail(MARL_ERR_CAPACITY, "%u cells, buffer holds %u", n, cap);
+    std::vector<float> rows((size_t)MARL_S_RECEPTORS * n);
+    for (int i = 0; i < MARL_S_RECEPTORS && n; ++i)
+        CK(cudaMemcpyAsync(rows.data() + (size_t)i * n, c->receptor_act + (size_t)i * c->t.cap, (size_t)n * 4,
+                           cudaMemcpyDeviceToHost, c->stream));
+    marl_status st = sync_and_check(c);
+    if (st) return st;
+    for (uint32_t j = 0; j < n; ++j)
+        for (int i = 0; i < MARL_S_RECEPTORS; ++i) out[(size_t)j * MARL_S_RECEPTORS + i] = rows[(size_t)i * n + j];
+    c->d2h_bytes += rows.size() * 4;
     return MARL_OK;
 }
 

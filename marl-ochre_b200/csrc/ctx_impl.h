@@ -39,6 +39,7 @@ struct marl_ctx {
     int32_t hold_cell = -1;    // marl_ctx_test_hold_dependency: cell, face and slot for the next phase
     int hold_face = 0;
     uint32_t hold_slot = 0;
+    float* receptor_act = nullptr;  // [8][cap] receptor activations of the last cell phase (optional output)
     uint32_t n = 0;
     uint32_t epoch = 0;
     bool schedule_dirty = true;

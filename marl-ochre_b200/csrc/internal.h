@@ -150,6 +150,7 @@ struct CellLaunch {
     uint32_t epoch;
     uint32_t* ticket;
     uint32_t* err;
+    float* act = nullptr;  // receptor activations [8][cap] of the cells updated (nullable)
 };
 
 cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s);
@@ -184,6 +185,11 @@ cudaError_t launch_moves(CellTable t, const uint32_t* dst, const uint32_t* src, 
                          int32_t* cmap, cudaStream_t s);
 cudaError_t launch_rebuild_maps(const CellTable& t, uint32_t n, const Grid& g, int32_t* cmap, uint8_t* mask,
                                 cudaStream_t s);
+
+// ---- horizontal gene transfer (hgt.cu) ----
+// items: (donor, recipient, pair index, 0), one conflict-free wave.
+cudaError_t launch_hgt(const CellTable& t, const uint4* items, uint32_t count, uint64_t seed, uint64_t tick,
+                       cudaStream_t s);
 
 // ---- device fate (fate.cu) ----
 // Scalars of a context's device fate processing.  While the context runs

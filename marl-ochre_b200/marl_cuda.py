@@ -218,7 +218,8 @@ EXPORTED = [
     "marl_sim_params_default", "marl_last_error", "marl_abi_version",
     "marl_ctx_create", "marl_ctx_destroy", "marl_ctx_set_stream", "marl_ctx_set_params", "marl_ctx_synchronize",
     "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_set_cell_lanes", "marl_ctx_set_wait_limit",
-    "marl_ctx_test_hold_dependency", "marl_ctx_autotune", "marl_ctx_counters",
+    "marl_ctx_test_hold_dependency", "marl_ctx_set_receptor_output", "marl_ctx_download_receptor_activations",
+    "marl_ctx_hgt", "marl_ctx_autotune", "marl_ctx_counters",
     "marl_upload_field", "marl_download_field", "marl_upload_light", "marl_download_light",
     "marl_upload_cells", "marl_download_cells", "marl_cell_count", "marl_download_occupancy",
     "marl_apply_boundary_sources", "marl_diffuse", "marl_light_update", "marl_cell_phase", "marl_tick",
@@ -270,6 +271,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_set_cell_lanes": (c_int32, [P, c_uint32]),
         "marl_ctx_set_wait_limit": (c_int32, [P, c_uint32]),
         "marl_ctx_test_hold_dependency": (c_int32, [P, c_uint32, c_uint32, c_uint32]),
+        "marl_ctx_set_receptor_output": (c_int32, [P, c_int32]),
+        "marl_ctx_download_receptor_activations": (c_int32, [P, P, c_uint32, POINTER(c_uint32)]),
+        "marl_ctx_hgt": (c_int32, [P, P, P, c_uint32, c_uint64, c_uint64]),
         "marl_ctx_autotune": (c_int32, [P, c_int32, POINTER(c_float)]),
         "marl_ctx_counters": (c_int32, [P, POINTER(Counters)]),
         "marl_upload_field": (c_int32, [P, P]),
@@ -436,6 +440,28 @@ class Context:
 
     def set_tile(self, tile: int, zc: int) -> None:
         _check(self.lib.marl_ctx_set_tile(self.h, tile, zc), "marl_ctx_set_tile")
+
+    def set_receptor_output(self, enable: bool = True) -> None:
+        """Phase 1 (receptor activations) as an output of every later cell phase."""
+        _check(self.lib.marl_ctx_set_receptor_output(self.h, 1 if enable else 0), "marl_ctx_set_receptor_output")
+
+    def receptor_activations(self) -> np.ndarray:
+        """The last cell phase's receptor activations, [n][8]."""
+        n = self.cell_count()
+        out = np.zeros((max(n, 1), 8), np.float32)
+        got = c_uint32()
+        _check(self.lib.marl_ctx_download_receptor_activations(self.h, _ptr(out), out.shape[0], ctypes.byref(got)),
+               "marl_ctx_download_receptor_activations")
+        return out[: got.value]
+
+    def hgt(self, donors, recipients, seed: int, tick: int) -> None:
+        """transfer_reaction for each (donor, recipient) pair, in order."""
+        d = np.ascontiguousarray(donors, np.uint32)
+        r = np.ascontiguousarray(recipients, np.uint32)
+        if d.shape != r.shape:
+            raise ValueError("donors and recipients differ in length")
+        _check(self.lib.marl_ctx_hgt(self.h, _ptr(d) if d.size else None, _ptr(r) if r.size else None, d.size,
+                                     seed, tick), "marl_ctx_hgt")
 
     def set_wait_limit(self, polls: int) -> None:
         """Polls of an unfinished dependency before a cell gives up (0: default)."""

@@ -354,6 +354,43 @@ int cell_tick(marl_cell& cell, T* internal, const T ext[12], T light, const marl
     return event;
 }
 
+// Phase 1 of CellState::tick (crates/marl-cell/src/cell.rs:206-220): the Hill
+// activation of receptor i from the gathered species i.  The reference keeps
+// the result in `_activation`, which nothing reads yet.
+void receptor_activations(const marl_cell& cell, const float ext[12], const marl_sim_params& sim, float act[8]) {
+    for (int i = 0; i < MARL_S_RECEPTORS; ++i) {
+        act[i] = 0.0f;
+        const marl_receptor_params& r = cell.ruleset.receptors[i];
+        if (i < MARL_S_EXT && std::fabs(r.gain) > sim.active_reaction_threshold) {
+            const float c = ext[i];
+            const float k = std::fmax(r.k_half, 1e-6f);
+            const float n = rclamp(r.n_hill, sim.hill_exponent_clamp_low, sim.hill_exponent_clamp_high);
+            const float kn = powf(k, n);
+            const float cn = powf(std::fmax(c, 0.0f), n);
+            act[i] = r.gain * cn / (kn + cn + 1e-9f);
+        }
+    }
+}
+
+// crates/marl-cell/src/hgt.rs:7-27 (transfer_reaction): a random active
+// reaction of the donor replaces the recipient's first inactive slot, or a
+// random slot when every slot is active.
+template <class R>
+void transfer_reaction(const marl_ruleset& donor, marl_ruleset& recipient, R& rng) {
+    int active[MARL_R_MAX];
+    int na = 0;
+    for (int i = 0; i < MARL_R_MAX; ++i)
+        if (std::fabs(donor.reactions[i].v_max) > 1e-9f) active[na++] = i;
+    if (na == 0) return;
+    const int donor_idx = active[rng.range(0, (uint32_t)na)];
+    const marl_reaction donated = donor.reactions[donor_idx];
+    int target = -1;
+    for (int i = 0; i < MARL_R_MAX && target < 0; ++i)
+        if (std::fabs(recipient.reactions[i].v_max) < 1e-9f) target = i;
+    if (target < 0) target = (int)rng.range(0, MARL_R_MAX);
+    recipient.reactions[target] = donated;
+}
+
 // -------------------------------------------------------------- spatial ----
 
 // crates/marl-sim/src/spatial.rs:8-15
@@ -876,6 +913,37 @@ void oracle_cell_phase_f32(float* field, const float* light, marl_cell* cells, u
         apply_deltas_to_neighbors(c.pos, field, cmap.data(), g, deltas);
     }
 }
+// The same loop, also returning each cell's receptor activations (phase 1,
+// from the environment it gathered), act_out [n][8].
+void oracle_cell_phase_act_f32(float* field, const float* light, marl_cell* cells, uint32_t n, int X, int Y, int Z,
+                               const marl_sim_params* p, int32_t* events_out, float* act_out) {
+    const Dims g{X, Y, Z};
+    std::vector<int32_t> cmap(g.V(), -1);
+    for (uint32_t i = 0; i < n; ++i) cmap[g.vox(cells[i].pos[0], cells[i].pos[1], cells[i].pos[2])] = (int32_t)i;
+    for (uint32_t i = 0; i < n; ++i) {
+        marl_cell& c = cells[i];
+        float ext[12], deltas[12];
+        read_neighbor_environment(c.pos, field, cmap.data(), g, ext);
+        receptor_activations(c, ext, *p, act_out + (size_t)i * 8);
+        const float l = light[g.vox(c.pos[0], c.pos[1], c.pos[2])];
+        const int ev = cell_tick<float>(c, c.internal, ext, l, *p, deltas);
+        if (events_out) events_out[i] = ev;
+        apply_deltas_to_neighbors(c.pos, field, cmap.data(), g, deltas);
+    }
+}
+
+// Horizontal gene transfer over pairs in order: pair k moves a reaction from
+// cells[donor[k]] to cells[recipient[k]] with its own stream, FateRng keyed by
+// (seed ^ kHgtSalt, tick, k).
+void oracle_hgt(marl_cell* cells, uint32_t n, const uint32_t* donor, const uint32_t* recipient, uint32_t pairs,
+                uint64_t seed, uint64_t tick) {
+    for (uint32_t k = 0; k < pairs; ++k) {
+        if (donor[k] >= n || recipient[k] >= n) continue;
+        FateRng rng(seed ^ 0x4847545452414E53ull, tick, k);  // "HGTTRANS"
+        transfer_reaction(cells[donor[k]].ruleset, cells[recipient[k]].ruleset, rng);
+    }
+}
+
 // Same loop in FP64 (field, light and internals in double); internal_out is
 // [n][16].  Cell fate flags are updated in `cells` as well.
 void oracle_cell_phase_f64(double* field, const double* light, marl_cell* cells, uint32_t n, int X, int Y, int Z,

@@ -52,6 +52,8 @@ def lib() -> ctypes.CDLL:
         "oracle_cell_tick": (c_int, [P, P, c_float, sp, P]),
         "oracle_cell_phase_f32": (None, [P, P, P, c_uint32, c_int, c_int, c_int, sp, P]),
         "oracle_cell_phase_f64": (None, [P, P, P, c_uint32, c_int, c_int, c_int, sp, P]),
+        "oracle_cell_phase_act_f32": (None, [P, P, P, c_uint32, c_int, c_int, c_int, sp, P, P]),
+        "oracle_hgt": (None, [P, c_uint32, P, P, c_uint32, c_uint64, c_uint64]),
         "oracle_mutate": (None, [P, P, sp]),
         "oracle_rng_seed": (None, [c_uint64, P]),
         "oracle_rng_next_u64": (c_uint64, [P]),
@@ -173,6 +175,29 @@ def cell_phase(field: np.ndarray, light_arr: np.ndarray, cells: np.ndarray, dims
     lib().oracle_cell_phase_f32(_p(f), _p(l), _p(c) if c.size else None, c.size, X, Y, Z, ctypes.byref(params),
                                 _p(ev))
     return f, c, ev[: c.size]
+
+
+def cell_phase_act(field: np.ndarray, light_arr: np.ndarray, cells: np.ndarray, dims, params: SimParams):
+    """The sequential cell loop plus each cell's receptor activations (cell.rs:206-220);
+    returns (field, cells, events, activations [n][8])."""
+    X, Y, Z = dims
+    f = np.ascontiguousarray(field, np.float32).copy()
+    l = np.ascontiguousarray(light_arr, np.float32)
+    c = np.ascontiguousarray(cells, CELL_DTYPE).copy()
+    ev = np.zeros(max(c.size, 1), np.int32)
+    act = np.zeros((max(c.size, 1), 8), np.float32)
+    lib().oracle_cell_phase_act_f32(_p(f), _p(l), _p(c) if c.size else None, c.size, X, Y, Z, ctypes.byref(params),
+                                    _p(ev), _p(act))
+    return f, c, ev[: c.size], act[: c.size]
+
+
+def hgt(cells: np.ndarray, donors, recipients, seed: int, tick: int) -> np.ndarray:
+    """transfer_reaction (crates/marl-cell/src/hgt.rs:7-27) for each (donor, recipient) pair in order."""
+    c = np.ascontiguousarray(cells, CELL_DTYPE).copy()
+    d = np.ascontiguousarray(donors, np.uint32)
+    r = np.ascontiguousarray(recipients, np.uint32)
+    lib().oracle_hgt(_p(c), c.size, _p(d) if d.size else None, _p(r) if r.size else None, d.size, seed, tick)
+    return c
 
 
 def cell_phase_f64(field: np.ndarray, light_arr: np.ndarray, cells: np.ndarray, dims, params: SimParams):
