@@ -233,7 +233,9 @@ def diffusion_roofline(marl, torch, engine, stream, fixed_tile=None) -> dict:
         tr = traffic.get("dram_bytes_per_launch")
     ctx.close()
     tiles = ["16x8 (4 stages)", "16x16 (4 stages)", "16x4 (4 stages)", "16x32 (4 stages)",
-             "16x8 (3 stages)", "16x16 (3 stages)", "16x4 (3 stages)", "16x32 (3 stages)"]
+             "16x8 (3 stages)", "16x16 (3 stages)", "16x4 (3 stages)", "16x32 (3 stages)",
+             "16x4 (3 stages, direct stores)", "16x8 (3 stages, direct stores)",
+             "16x16 (3 stages, direct stores)", "16x32 (3 stages, direct stores)"]
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tr, "kernel": "k_diffuse (diffusion substep, TMA z-march)", "peak_source": src,
             "algorithmic_bytes_per_launch": bytes_per_launch, "us_per_launch": t_sub * 1e6,

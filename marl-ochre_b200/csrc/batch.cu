@@ -979,7 +979,7 @@ marl_status marl_batch_autotune(marl_batch* b, int32_t reps, float* best_us_out)
     if (reps < 1) reps = 3;
     int maxZ = 0;
     for (auto& R : b->runs) maxZ = std::max(maxZ, R.g.Z);
-    const int zcs[] = {4, 8, 16, 32, 64};
+    const int zcs[] = {4, 8, 10, 12, 13, 16, 21, 32, 64};  // 10-21: chunk counts that fill the SMs on common Z
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

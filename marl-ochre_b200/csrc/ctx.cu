@@ -610,7 +610,7 @@ marl_status marl_ctx_get_tile(marl_ctx* c, int32_t* tile, int32_t* zc) {
 marl_status marl_ctx_autotune(marl_ctx* c, int32_t reps, float* best_us_out) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
     if (reps < 1) reps = 3;
-    const int zcs[] = {4, 8, 16, 32, 64};
+    const int zcs[] = {4, 8, 10, 12, 13, 16, 21, 32, 64};  // 10-21: chunk counts that fill the SMs on common Z
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

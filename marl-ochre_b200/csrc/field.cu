@@ -67,7 +67,12 @@ __global__ void k_sources(float* __restrict__ f, Grid g, FieldConsts k) {
 #endif
 constexpr int kDiffTX = 16;
 
-template <int TY, int STAGES>
+// DIRECT: results go from registers straight to global memory (coalesced
+// 16-byte stores) instead of through a triple-buffered shared tile and a TMA
+// store, and the xy neighbours are read one species pair at a time.  That
+// drops OUT_BUFS * OUT_BYTES of shared memory and about 40 live registers per
+// thread, so more CTAs fit on an SM; the autotuner decides per grid.
+template <int TY, int STAGES, bool DIRECT = false>
 struct DiffTile {
     static constexpr int TX = kDiffTX;
     static constexpr int PW = TX + 2, PH = TY + 2;
@@ -79,7 +84,7 @@ struct DiffTile {
     static constexpr int PLANE_REGION = (PLANE_BYTES + 127) / 128 * 128;
     static constexpr int STAGE_BYTES = MASK_REGION + PLANE_REGION;
     static constexpr int OUT_BYTES = TY * TX * 48;
-    static constexpr int OUT_BUFS = 3;
+    static constexpr int OUT_BUFS = DIRECT ? 0 : 3;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + OUT_BUFS * OUT_BYTES + STAGES * 8;
     static_assert(ROWF <= 256 && TX * 12 <= 256 && PH <= 256 && MW <= 256, "TMA box dims are limited to 256");
     static_assert(OUT_BYTES % 128 == 0, "output staging alignment");
@@ -187,6 +192,36 @@ __device__ __forceinline__ void stencil(float out[12], const Vox& c, const Vox& 
 
 }
 
+// The same update with the four xy neighbours read from the staged plane one
+// species pair at a time (8-byte shared loads) instead of as whole voxels:
+// bit-identical, fewer live registers.  Packed adds, scalar multiplies, as
+// stencil() does.
+__device__ __forceinline__ void stencil_pairwise(float out[12], const Vox& c, const float* xm, const float* xp,
+                                                 const float* ym, const float* yp, const Vox& below,
+                                                 const Vox& above, bool wzm, bool wzp, const FieldConsts& k) {
+    const float structural = c.v[3].y;  // species 7
+    const float niche = 1.0f - div_rn(k.alpha_eps * structural, k.k_eps + structural);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const float2 cc = c.v[q];
+        const float2 zm = wzm ? cc : below.v[q];
+        const float2 zp = wzp ? cc : above.v[q];
+        const float2 d = make_float2(__fmul_rn(k.d_voxel[2 * q], niche), __fmul_rn(k.d_voxel[2 * q + 1], niche));
+        float2 lap = add2_rn(reinterpret_cast<const float2*>(xm)[q], reinterpret_cast<const float2*>(xp)[q]);
+        lap = add2_rn(lap, reinterpret_cast<const float2*>(ym)[q]);
+        lap = add2_rn(lap, reinterpret_cast<const float2*>(yp)[q]);
+        lap = add2_rn(lap, zm);
+        lap = add2_rn(lap, zp);
+        lap = add2_rn(lap, make_float2(__fmul_rn(-6.0f, cc.x), __fmul_rn(-6.0f, cc.y)));
+        const float2 ndecay = make_float2(__fmul_rn(-k.lambda_decay[2 * q], cc.x),
+                                          __fmul_rn(-k.lambda_decay[2 * q + 1], cc.y));
+        const float2 t = add2_rn(make_float2(__fmul_rn(d.x, lap.x), __fmul_rn(d.y, lap.y)), ndecay);
+        const float2 nc = add2_rn(cc, make_float2(__fmul_rn(k.dt_sub, t.x), __fmul_rn(k.dt_sub, t.y)));
+        out[2 * q] = fmaxf(nc.x, 0.0f);
+        out[2 * q + 1] = fmaxf(nc.y, 0.0f);
+    }
+}
+
 // crates/marl-field/src/field.rs:107-203 (Field::diffusion_step_inner).
 //
 // 2.5D z-marching stencil.  A CTA owns a 16 x TY column tile and a chunk of
@@ -200,13 +235,15 @@ __device__ __forceinline__ void stencil(float out[12], const Vox& c, const Vox& 
 // the four xy neighbours come from the staged plane, and the wall flags of
 // the next plane are read one plane early so the neighbour loads never wait
 // on them.  Results go to a triple-buffered shared tile; one TMA bulk-tensor
-// store per plane writes it back.  One barrier per plane.
-template <int TY, int STAGES>
+// store per plane writes it back (with DIRECT, coalesced 16-byte stores from
+// registers into dst_field).  One barrier per plane.
+template <int TY, int STAGES, bool DIRECT>
 __device__ __forceinline__ void diffuse_tile(const CUtensorMap* tm_src, const CUtensorMap* tm_dst,
                                              const CUtensorMap* tm_mask, const Grid g, const int bx, const int by,
                                              const int bz, const int zc, const FieldConsts& k, const int apply_sources,
-                                             float* __restrict__ c4_out, uint32_t* __restrict__ err) {
-    using T = DiffTile<TY, STAGES>;
+                                             float* __restrict__ c4_out, uint32_t* __restrict__ err,
+                                             float* __restrict__ dst_field) {
+    using T = DiffTile<TY, STAGES, DIRECT>;
     constexpr int TX = T::TX;
     extern __shared__ __align__(128) unsigned char smem[];
     float* outbuf = reinterpret_cast<float*>(smem + STAGES * T::STAGE_BYTES);
@@ -334,29 +371,46 @@ __device__ __forceinline__ void diffuse_tile(const CUtensorMap* tm_src, const CU
             const float* P = plane_of(p);
             // A wall or occupied neighbour reads as the centre value: point
             // its load at the centre voxel.
-            Vox xm, xp, ym, yp;
-            load_vox(xm, P + ci - ((walls & 1u) ? 0 : 12));
-            load_vox(xp, P + ci + ((walls & 2u) ? 0 : 12));
-            load_vox(ym, P + ci - ((walls & 4u) ? 0 : T::ROWF));
-            load_vox(yp, P + ci + ((walls & 8u) ? 0 : T::ROWF));
-            stencil(out, C, xm, xp, ym, yp, B, A, z == 0 || mB, z >= g.Z - 1 || mA, k);
+            if constexpr (DIRECT) {
+                stencil_pairwise(out, C, P + ci - ((walls & 1u) ? 0 : 12), P + ci + ((walls & 2u) ? 0 : 12),
+                                 P + ci - ((walls & 4u) ? 0 : T::ROWF), P + ci + ((walls & 8u) ? 0 : T::ROWF), B, A,
+                                 z == 0 || mB, z >= g.Z - 1 || mA, k);
+            } else {
+                Vox xm, xp, ym, yp;
+                load_vox(xm, P + ci - ((walls & 1u) ? 0 : 12));
+                load_vox(xp, P + ci + ((walls & 2u) ? 0 : 12));
+                load_vox(ym, P + ci - ((walls & 4u) ? 0 : T::ROWF));
+                load_vox(yp, P + ci + ((walls & 8u) ? 0 : T::ROWF));
+                stencil(out, C, xm, xp, ym, yp, B, A, z == 0 || mB, z >= g.Z - 1 || mA, k);
+            }
         }
-        float* ob = outbuf + (p % 3) * (T::OUT_BYTES / 4) + (ty * TX + tx) * 12;
-        reinterpret_cast<float4*>(ob)[0] = make_float4(out[0], out[1], out[2], out[3]);
-        reinterpret_cast<float4*>(ob)[1] = make_float4(out[4], out[5], out[6], out[7]);
-        reinterpret_cast<float4*>(ob)[2] = make_float4(out[8], out[9], out[10], out[11]);
+        if constexpr (DIRECT) {
+            if (active) {
+                float4* dst = reinterpret_cast<float4*>(dst_field + (((size_t)z * g.Y + y) * g.X + x) * 12);
+                __stcg(dst, make_float4(out[0], out[1], out[2], out[3]));
+                __stcg(dst + 1, make_float4(out[4], out[5], out[6], out[7]));
+                __stcg(dst + 2, make_float4(out[8], out[9], out[10], out[11]));
+            }
+        } else {
+            float* ob = outbuf + (p % 3) * (T::OUT_BYTES / 4) + (ty * TX + tx) * 12;
+            reinterpret_cast<float4*>(ob)[0] = make_float4(out[0], out[1], out[2], out[3]);
+            reinterpret_cast<float4*>(ob)[1] = make_float4(out[4], out[5], out[6], out[7]);
+            reinterpret_cast<float4*>(ob)[2] = make_float4(out[8], out[9], out[10], out[11]);
+        }
         if (c4_out && active) c4_out[((size_t)z * g.Y + y) * g.X + x] = out[4];
         walls = next_walls;
-        fence_proxy_async_smem();
+        if constexpr (!DIRECT) fence_proxy_async_smem();
         __syncthreads();
         if (s_abort[p & 1]) {
             aborted = true;
             return false;
         }
-        if (tid == 0) {
-            tma_store_3d(tm_dst, outbuf + (p % 3) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
-            bulk_commit();
-            bulk_wait_read<1>();  // the store of plane p-1 has read its buffer
+        if constexpr (!DIRECT) {
+            if (tid == 0) {
+                tma_store_3d(tm_dst, outbuf + (p % 3) * (T::OUT_BYTES / 4), x0 * 12, y0, z);
+                bulk_commit();
+                bulk_wait_read<1>();  // the store of plane p-1 has read its buffer
+            }
         }
         return true;
     };
@@ -373,7 +427,7 @@ __device__ __forceinline__ void diffuse_tile(const CUtensorMap* tm_src, const CU
     }
 
     if (tid == 0) {
-        bulk_wait_all();
+        if constexpr (!DIRECT) bulk_wait_all();
         // After an abort, wait (bounded) for loads still in flight so no copy
         // lands in shared memory after the CTA exits.
         if (aborted)
@@ -381,30 +435,38 @@ __device__ __forceinline__ void diffuse_tile(const CUtensorMap* tm_src, const CU
     }
 }
 
-template <int TY, int STAGES>
-__global__ void __launch_bounds__(kDiffTX* TY) k_diffuse(const __grid_constant__ CUtensorMap tm_src,
-                                                        const __grid_constant__ CUtensorMap tm_dst,
-                                                        const __grid_constant__ CUtensorMap tm_mask, Grid g, int zc,
-                                                        FieldConsts k, int apply_sources, float* __restrict__ c4_out,
-                                                        uint32_t* __restrict__ err) {
-    diffuse_tile<TY, STAGES>(&tm_src, &tm_dst, &tm_mask, g, blockIdx.x, blockIdx.y, blockIdx.z, zc, k, apply_sources,
-                             c4_out, err);
+// Resident CTAs per SM each form is compiled for, which sets its register
+// budget: 128 registers a thread for the staged-store tiles, 96-102 for the
+// direct-store tiles of 4 and 8 rows.
+template <int TY, bool DIRECT>
+constexpr int diff_min_blocks() {
+    return DIRECT ? (TY <= 4 ? 10 : (TY <= 8 ? 5 : (TY <= 16 ? 2 : 1)))
+                  : (TY <= 4 ? 8 : (TY <= 8 ? 4 : (TY <= 16 ? 2 : 1)));
+}
+
+template <int TY, int STAGES, bool DIRECT>
+__global__ void __launch_bounds__(kDiffTX* TY, (diff_min_blocks<TY, DIRECT>()))
+    k_diffuse(const __grid_constant__ CUtensorMap tm_src, const __grid_constant__ CUtensorMap tm_dst,
+              const __grid_constant__ CUtensorMap tm_mask, Grid g, int zc, FieldConsts k, int apply_sources,
+              float* __restrict__ c4_out, uint32_t* __restrict__ err, float* __restrict__ dst_field) {
+    diffuse_tile<TY, STAGES, DIRECT>(&tm_src, &tm_dst, &tm_mask, g, blockIdx.x, blockIdx.y, blockIdx.z, zc, k,
+                                     apply_sources, c4_out, err, dst_field);
 }
 
 // Batched form: one launch advances one substep of every run.  CTA b owns
 // work item items[b] = (run, tile x, tile y, z-chunk); the run's tensor maps
 // (loads from buffer 0/1, stores into buffer 0/1, mask) are read from global
 // memory.  All runs share the ping-pong parity of the substep.
-template <int TY, int STAGES>
-__global__ void __launch_bounds__(kDiffTX* TY)
+template <int TY, int STAGES, bool DIRECT>
+__global__ void __launch_bounds__(kDiffTX* TY, (diff_min_blocks<TY, DIRECT>()))
     k_diffuse_batch(const RunDesc* __restrict__ runs, const CUtensorMap* __restrict__ maps,
                     const int4* __restrict__ items, int zc, FieldConsts k, int parity, int apply_sources, int emit_c4,
                     uint32_t* __restrict__ err) {
     const int4 it = items[blockIdx.x];
     const RunDesc& r = runs[it.x];
     const CUtensorMap* m = maps + (size_t)it.x * kMapsPerRun;
-    diffuse_tile<TY, STAGES>(&m[parity], &m[2 + (parity ^ 1)], &m[4], r.g, it.y, it.z, it.w, zc, k, apply_sources,
-                             emit_c4 ? r.c4 : nullptr, err);
+    diffuse_tile<TY, STAGES, DIRECT>(&m[parity], &m[2 + (parity ^ 1)], &m[4], r.g, it.y, it.z, it.w, zc, k,
+                                     apply_sources, emit_c4 ? r.c4 : nullptr, err, r.field[parity ^ 1]);
 }
 
 // ------------------------------------------------------------ light ------
@@ -574,26 +636,29 @@ __global__ void k_unpack_mask(const uint8_t* __restrict__ mask, uint8_t* __restr
 
 // ======================================================== launchers ======
 
-// Tile table: (rows per tile, plane stages).  The autotuner picks one.
-static const int kTileTY[] = {8, 16, 4, 32, 8, 16, 4, 32};  // stages: 4 for tiles 0-3, 3 for 4-7
+// Tile table: (rows per tile, plane stages, store form).  The autotuner picks
+// one.  Tiles 0-3: 4 stages, 4-7: 3 stages, both through a shared output tile
+// and a TMA store; 8-11: 3 stages, direct stores.
+static const int kTileTY[] = {8, 16, 4, 32, 8, 16, 4, 32, 4, 8, 16, 32};
 
-int diffusion_tile_count() { return 8; }
+int diffusion_tile_count() { return 12; }
 
 void diffusion_tile_shape(int tile, int* tx, int* ty) {
     *tx = kDiffTX;
     *ty = kTileTY[tile];
 }
 
-template <int TY, int STAGES>
+template <int TY, int STAGES, bool DIRECT = false>
 static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
                                     int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
-    using T = DiffTile<TY, STAGES>;
+    using T = DiffTile<TY, STAGES, DIRECT>;
     static std::atomic<int> setup[kSetupDevices];
-    cudaError_t e = set_smem_once(setup, k_diffuse<TY, STAGES>, T::SMEM_BYTES);
+    cudaError_t e = set_smem_once(setup, k_diffuse<TY, STAGES, DIRECT>, T::SMEM_BYTES);
     if (e != cudaSuccess) return e;
     dim3 grid((g.X + kDiffTX - 1) / kDiffTX, (g.Y + TY - 1) / TY, (g.Z + plan.zc - 1) / plan.zc);
-    k_diffuse<TY, STAGES><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(
-        plan.tm_load[which_src], plan.tm_store[which_src ^ 1], plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err);
+    k_diffuse<TY, STAGES, DIRECT><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(
+        plan.tm_load[which_src], plan.tm_store[which_src ^ 1], plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err,
+        plan.buf[which_src ^ 1]);
     return cudaGetLastError();
 }
 
@@ -607,21 +672,25 @@ cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const Grid&
         case 4: return launch_diffuse_t<8, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
         case 5: return launch_diffuse_t<16, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
         case 6: return launch_diffuse_t<4, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
-        default: return launch_diffuse_t<32, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 7: return launch_diffuse_t<32, 3>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 8: return launch_diffuse_t<4, 3, true>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 9: return launch_diffuse_t<8, 3, true>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        case 10: return launch_diffuse_t<16, 3, true>(plan, which_src, g, k, apply_sources, c4_out, err, s);
+        default: return launch_diffuse_t<32, 3, true>(plan, which_src, g, k, apply_sources, c4_out, err, s);
     }
 }
 
-template <int TY, int STAGES>
+template <int TY, int STAGES, bool DIRECT = false>
 static cudaError_t launch_diffuse_batch_t(const RunDesc* runs, const CUtensorMap* maps, const int4* items, int n_items,
                                           int zc, const FieldConsts& k, int parity, int apply_sources, int emit_c4,
                                           uint32_t* err, cudaStream_t s) {
-    using T = DiffTile<TY, STAGES>;
+    using T = DiffTile<TY, STAGES, DIRECT>;
     if (n_items == 0) return cudaSuccess;
     static std::atomic<int> setup[kSetupDevices];
-    cudaError_t e = set_smem_once(setup, k_diffuse_batch<TY, STAGES>, T::SMEM_BYTES);
+    cudaError_t e = set_smem_once(setup, k_diffuse_batch<TY, STAGES, DIRECT>, T::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    k_diffuse_batch<TY, STAGES><<<n_items, kDiffTX * TY, T::SMEM_BYTES, s>>>(runs, maps, items, zc, k, parity,
-                                                                           apply_sources, emit_c4, err);
+    k_diffuse_batch<TY, STAGES, DIRECT><<<n_items, kDiffTX * TY, T::SMEM_BYTES, s>>>(runs, maps, items, zc, k, parity,
+                                                                                   apply_sources, emit_c4, err);
     return cudaGetLastError();
 }
 
@@ -636,7 +705,11 @@ cudaError_t launch_diffuse_batch(int tile, const RunDesc* runs, const CUtensorMa
         case 4: return launch_diffuse_batch_t<8, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
         case 5: return launch_diffuse_batch_t<16, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
         case 6: return launch_diffuse_batch_t<4, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
-        default: return launch_diffuse_batch_t<32, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 7: return launch_diffuse_batch_t<32, 3>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 8: return launch_diffuse_batch_t<4, 3, true>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 9: return launch_diffuse_batch_t<8, 3, true>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        case 10: return launch_diffuse_batch_t<16, 3, true>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
+        default: return launch_diffuse_batch_t<32, 3, true>(runs, maps, items, n_items, zc, k, parity, apply_sources, emit_c4, err, s);
     }
 }
 
@@ -725,6 +798,8 @@ bool plan_diffusion(DiffusionPlan* plan, const float* a, const float* b, const u
     diffusion_tile_shape(tile, &tx, &ty);
     plan->tile = tile;
     plan->zc = zc > 0 ? zc : 16;
+    plan->buf[0] = const_cast<float*>(a);
+    plan->buf[1] = const_cast<float*>(b);
     const float* bufs[2] = {a, b};
     for (int i = 0; i < 2; ++i) {
         if (!encode_field_map(&plan->tm_load[i], bufs[i], g, tx + 2, ty + 2)) return false;

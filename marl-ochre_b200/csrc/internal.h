@@ -17,6 +17,7 @@ struct DiffusionPlan {
     CUtensorMap tm_load[2];   // halo'd plane loads from buffer 0 / buffer 1
     CUtensorMap tm_store[2];  // tile stores into buffer 0 / buffer 1
     CUtensorMap tm_mask;
+    float* buf[2] = {nullptr, nullptr};  // the two buffers (direct-store tiles write into them)
     int tile = 0;  // index into the tile-shape table
     int zc = 16;   // z-chunk per CTA
 };

@@ -61,8 +61,12 @@ def test_diffusion_every_tile_ragged(marl, oracle_mod, dims):
     oracle_mod.diffuse(cpu, occ, dims, p, 3)
     ctx = ctx_with(marl, dims, p, cells_at(marl, occ), f0, cap=max(int(occ.sum()), 1))
     lib = marl.load()
-    for tile in range(4):
-        for zc in (1, 4, 16):
+    tiles = 0
+    while lib.marl_ctx_set_tile(ctx.h, tiles, 4) == 0:  # every tile shape the library offers
+        tiles += 1
+    assert tiles >= 12
+    for tile in range(tiles):
+        for zc in (1, 4, 13, 16):
             assert lib.marl_ctx_set_tile(ctx.h, tile, zc) == 0
             ctx.upload_field(f0)
             ctx.diffuse(3)
