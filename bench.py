@@ -303,10 +303,12 @@ def ensemble_leg(marl, torch, stream, ticks: int = 1000, window: int = 20, surro
     tick-`ticks` state, `window` more plain ticks and then, with a trained
     surrogate, `window` ticks gated at 1e-3; and the same ensemble with fate on
     the device, `ticks` ticks from seeding."""
-    runs = [(ENSEMBLE_GRIDS[i // 16], i) for i in range(64)]
+    # Table capacity: half the voxels of the run's grid (the seeded runs hold
+    # about a quarter of their voxels at most by tick 1000).
+    runs = [(g, i, SEED_COUNT, g[0] * g[1] * g[2] // 2) for i, g in ((i, ENSEMBLE_GRIDS[i // 16]) for i in range(64))]
 
     def make(device_fate):
-        b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT, cell_capacity=0)
+        b = marl.Batch(runs, marl.default_params(), seed_count=SEED_COUNT)
         b.set_stream(stream.cuda_stream)
         us = b.autotune(3)
         if device_fate:

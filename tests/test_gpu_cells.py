@@ -13,7 +13,10 @@ from helpers import clustered_positions, random_cells, random_field
 pytestmark = pytest.mark.gpu
 
 
-def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32):
+FORMS = [1, 2]  # the latency and the throughput form of the plain cell loop (marl_ctx_set_cell_form)
+
+
+def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32, form=0):
     rng = np.random.default_rng(seed)
     X, Y, Z = dims
     f = random_field(dims, rng)
@@ -21,6 +24,7 @@ def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32):
     p = marl.default_params()
     ctx = marl.Context(dims, p, cell_capacity=max(len(cells), 1))
     marl._check(marl.load().marl_ctx_set_cell_lanes(ctx.h, lanes), "marl_ctx_set_cell_lanes")
+    ctx.set_cell_form(form)
     ctx.upload_field(f)
     ctx.upload_light(light)
     ctx.upload_cells(cells)
@@ -43,23 +47,25 @@ def assert_same(gpu, cpu):
     assert gc["ruleset"].tobytes() == cc["ruleset"].tobytes()
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("n", [1, 7, 300])
-def test_cell_phase_sparse(marl, oracle_mod, n):
+def test_cell_phase_sparse(marl, oracle_mod, n, form):
     dims = (32, 24, 16)
     cells = random_cells(dims, n, np.random.default_rng(n))
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, n)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, n, form=form)
     assert_same(gpu, cpu)
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("lanes", [1, 5, 8, 16])
-def test_cell_phase_cells_per_warp(marl, oracle_mod, lanes):
+def test_cell_phase_cells_per_warp(marl, oracle_mod, lanes, form):
     """Fewer cells per warp ticket (marl_ctx_set_cell_lanes) leave the result
     unchanged: dense blobs, long dependency chains."""
     dims = (24, 20, 16)
     rng = np.random.default_rng(31)
     pos = clustered_positions(dims, 0.5, rng, 1, 3)
     cells = random_cells(dims, len(pos), rng, positions=pos)
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 78, lanes=lanes)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 78, lanes=lanes, form=form)
     assert_same(gpu, cpu)
 
 
@@ -71,18 +77,20 @@ def test_cell_lanes_rejects_out_of_range(marl):
     assert lib.marl_ctx_set_cell_lanes(ctx.h, 32) == 0
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("frac", [0.05, 0.3, 0.7])
-def test_cell_phase_clustered(marl, oracle_mod, frac):
+def test_cell_phase_clustered(marl, oracle_mod, frac, form):
     """Clustered blobs: many cells share empty voxels, long dependency chains."""
     dims = (24, 20, 16)
     rng = np.random.default_rng(int(frac * 100))
     pos = clustered_positions(dims, frac, rng, 1, 3)
     cells = random_cells(dims, len(pos), rng, positions=pos)
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 77)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 77, form=form)
     assert_same(gpu, cpu)
 
 
-def test_cell_phase_chain_order(marl, oracle_mod):
+@pytest.mark.parametrize("form", FORMS)
+def test_cell_phase_chain_order(marl, oracle_mod, form):
     """Cells in a line with one-voxel gaps: every cell depends on its predecessor."""
     dims = (64, 1, 1)
     xs = np.arange(0, 64, 2)
@@ -90,16 +98,67 @@ def test_cell_phase_chain_order(marl, oracle_mod):
     order = rng.permutation(len(xs))  # scrambled Vec order
     pos = np.stack([xs[order], np.zeros_like(xs), np.zeros_like(xs)], 1)
     cells = random_cells(dims, len(pos), rng, positions=pos)
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 5)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 5, form=form)
     assert_same(gpu, cpu)
 
 
-def test_cell_phase_many_cells(marl, oracle_mod):
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_cell_phase_many_cells(marl, oracle_mod, form):
     """Cell-kinetics microbenchmark shape at reduced size: 11.9% random occupancy."""
     dims = (64, 64, 48)
     n = int(0.119 * 64 * 64 * 48)
     cells = random_cells(dims, n, np.random.default_rng(2024))
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 2024)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 2024, form=form)
+    assert_same(gpu, cpu)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("seed", [31, 32, 33])
+def test_cell_phase_edge_rulesets(marl, oracle_mod, form, seed):
+    """Rulesets that take every branch of the transport, reaction and effector
+    order: transporters and effectors sharing a species, invalid indices
+    (species out of range skip the slot), reactions whose cofactor is their
+    substrate or product, substrate equal to product, v_max exactly at the
+    threshold (runs, not counted active), cofactor indices out of range, and
+    cells dense enough to chain."""
+    dims = (20, 16, 12)
+    rng = np.random.default_rng(seed)
+    pos = clustered_positions(dims, 0.3, rng, 1, 3)
+    n = len(pos)
+    cells = random_cells(dims, n, rng, positions=pos)
+    rs = cells["ruleset"]
+    tp, rx, ef = rs["transport"], rs["reactions"], rs["effectors"]
+    tp["int_species"] = rng.integers(0, 4, (n, 8))          # few species: many transporters share one
+    tp["ext_species"] = rng.integers(0, 3, (n, 8))
+    bad = rng.random((n, 8)) < 0.15
+    tp["ext_species"][bad] = rng.integers(12, 256, bad.sum())
+    bad = rng.random((n, 8)) < 0.15
+    tp["int_species"][bad] = rng.integers(16, 256, bad.sum())
+    ef["int_species"] = rng.integers(0, 4, (n, 8))
+    ef["ext_species"] = rng.integers(0, 3, (n, 8))
+    ef["threshold"] = (0.3 * rng.random((n, 8))).astype(np.float32)
+    bad = rng.random((n, 8)) < 0.15
+    ef["int_species"][bad] = rng.integers(16, 256, bad.sum())
+    bad = rng.random((n, 8)) < 0.15
+    ef["ext_species"][bad] = rng.integers(12, 256, bad.sum())
+    rx["substrate"] = rng.integers(0, 5, (n, 16))
+    rx["product"] = rng.integers(0, 5, (n, 16))
+    rx["catalyst"] = rng.integers(0, 6, (n, 16))
+    cof = rng.integers(0, 5, (n, 16))
+    pick = rng.random((n, 16))
+    cof[pick < 0.2] = rx["substrate"][pick < 0.2]                       # cofactor = substrate
+    cof[(pick >= 0.2) & (pick < 0.4)] = rx["product"][(pick >= 0.2) & (pick < 0.4)]  # cofactor = product
+    cof[pick > 0.8] = 0xFF
+    cof[(pick > 0.75) & (pick <= 0.8)] = rng.integers(16, 255, ((pick > 0.75) & (pick <= 0.8)).sum())
+    rx["cofactor"] = cof
+    thr = marl.default_params().active_reaction_threshold
+    vm = rx["v_max"]
+    vm[rng.random((n, 16)) < 0.1] = np.float32(thr)
+    vm[rng.random((n, 16)) < 0.1] = np.float32(-thr)
+    vm[rng.random((n, 16)) < 0.1] = 0.0
+    bad = rng.random((n, 16)) < 0.05
+    rx["catalyst"][bad] = rng.integers(16, 256, bad.sum())
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, seed, form=form)
     assert_same(gpu, cpu)
 
 
