@@ -109,14 +109,16 @@ struct CellScratch {
     float4 fate[kTickThreads];
     float x[MARL_M_INT][kTickThreads];
     float ext[MARL_S_EXT][kTickThreads];
+    float del[MARL_S_EXT][kTickThreads];
 };
 constexpr int kTickSmem = (int)sizeof(CellScratch);
 
 // Per-thread state of the throughput form: only what is indexed dynamically
-// (the internal species and the gathered environment).
+// (the internal species, the gathered environment and the field deltas).
 struct LeanScratch {
     float x[MARL_M_INT][kTickThreads];
     float ext[MARL_S_EXT][kTickThreads];
+    float del[MARL_S_EXT][kTickThreads];
 };
 constexpr int kTickSmemLean = (int)sizeof(LeanScratch);
 
@@ -130,7 +132,6 @@ constexpr int kTickSmemLean = (int)sizeof(LeanScratch);
 // on an SM).  Both give the same bits: only where the values come from differs.
 struct StagedRules {
     const CellScratch& S;
-    static constexpr bool kStaged = true;
     __device__ __forceinline__ uint4 rx(int r) const { return S.rx[r][threadIdx.x]; }
     __device__ __forceinline__ float2 tp(int i) const { return S.tp[i][threadIdx.x]; }
     __device__ __forceinline__ float2 ef(int i) const { return S.ef[i][threadIdx.x]; }
@@ -141,7 +142,6 @@ struct StagedRules {
 struct TableRules {
     const CellTable& t;
     uint32_t j;
-    static constexpr bool kStaged = false;
     __device__ __forceinline__ uint4 rx(int r) const { return __ldg(&t.rx[(size_t)r * t.cap + j]); }
     __device__ __forceinline__ float2 tp(int i) const { return __ldg(&t.tp_rate[(size_t)i * t.cap + j]); }
     __device__ __forceinline__ float2 ef(int i) const { return __ldg(&t.ef_par[(size_t)i * t.cap + j]); }
@@ -149,6 +149,10 @@ struct TableRules {
     __device__ __forceinline__ uint4 ef_idx() const { return __ldg(&t.ef_idx[j]); }
     __device__ __forceinline__ float4 fate() const { return __ldg(&t.fate[j]); }
 };
+template <bool LEAN>
+using ScratchOf = typename std::conditional<LEAN, LeanScratch, CellScratch>::type;
+template <bool LEAN>
+using RulesOf = typename std::conditional<LEAN, TableRules, StagedRules>::type;
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
@@ -221,58 +225,14 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, Scr& S, uint32_
     pre.light = v.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
 }
 
-// Validity and species indices of transporter i (cell.rs:226-230): ext in the
-// low byte and internal in the high byte of its 16-bit pair.
-__device__ __forceinline__ void transporter(const uint32_t (&w)[4], int i, uint32_t& e, uint32_t& k, bool& valid) {
-    const uint32_t pair = (w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
-    e = pair & 0xFF;
-    k = pair >> 8;
-    valid = e < MARL_S_EXT && k < MARL_M_INT;
-}
-
-// Secretions the transporters would compute from the cell's state before its
-// update (cell.rs:231-232).  Transporter i's value holds when no earlier valid
-// transporter of the cell writes the same internal species (bit i of `first`):
-// until then that species is the staged one.  Computed while the cell waits
-// for its dependencies, so only the uptakes, which need the gathered
-// environment, remain after the wait; the others are recomputed in order.
-template <class Scr, class Rules>
-__device__ __forceinline__ void presecretions(const Scr& S, const Rules& R, float (&sec)[MARL_S_TRANSPORTERS],
-                                              uint32_t& first) {
-    const int tid = threadIdx.x;
-    const uint4 tpi = R.tp_idx();
-    const uint32_t tpw[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
-    uint32_t written = 0;  // internal species written by an earlier valid transporter
-    first = 0;
-#pragma unroll
-    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
-        uint32_t e, k;
-        bool valid;
-        transporter(tpw, i, e, k, valid);
-        sec[i] = 0.0f;
-        if (valid && !((written >> k) & 1u)) {
-            const float xk = S.x[k][tid];
-            sec[i] = div_rn(R.tp(i).y * xk, 1.0f + xk);
-            first |= 1u << i;
-        }
-        if (valid) written |= 1u << k;
-    }
-}
-
 // Gather and transport of cell j (spatial.rs:56-77, cell.rs:223-243): the
-// neighbour mean into S.ext, the transport deltas into del[], S.x the internal
-// state after transport with the light in slot 15.  Shared by the cell loop
-// and the surrogate's pre-pass, so both produce the same bits from the same
-// field.
-//
-// Transport keeps the reference's order exactly, but not through shared
-// memory: every transporter's internal species is read up front, and the
-// value an earlier transporter of the same species wrote is forwarded in
-// registers, so only transporters that share a species depend on each other.
+// neighbour mean into S.ext, S.del zeroed then holding the transport deltas,
+// S.x the internal state after transport with the light in slot 15.  Shared
+// by the cell loop and the surrogate's pre-pass, so both produce the same bits
+// from the same field.
 template <class Scr, class Rules>
 __device__ __forceinline__ void gather_transport(const CellRunView& v, const CellConsts& c, Scr& S, const Rules& R,
-                                                 const CellPre& pre, const float (&sec)[MARL_S_TRANSPORTERS],
-                                                 uint32_t first, float4 (&nv)[6][3], float (&del)[MARL_S_EXT]) {
+                                                 const CellPre& pre, float4 (&nv)[6][3]) {
     const int tid = threadIdx.x;
     const Grid g = v.g;
     const uint32_t nb = pre.nb;
@@ -313,46 +273,35 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
     for (int s = 0; s < 12; ++s) S.ext[s][tid] = acc[s];
 
     // CellState::tick (cell.rs:193-369).  Phase 1 (receptors) only writes an
-    // unused local; it is an optional output (receptor_activations).
+    // unused local and is omitted.
+#pragma unroll
+    for (int s = 0; s < 12; ++s) S.del[s][tid] = 0.0f;
     const float dt = c.dt;
+    cp_async_wait_all();
 
-    // Phase 2: transport (cell.rs:223-238).
+    // Phase 2: transport (cell.rs:223-238).  Uptake depends only on the
+    // gathered environment, so all eight are evaluated first; secretion
+    // follows the internal state transporter by transporter.
     const uint4 tpi = R.tp_idx();
     const uint32_t tpw[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
-    float2 rates[MARL_S_TRANSPORTERS];
-    uint32_t te[MARL_S_TRANSPORTERS], tk[MARL_S_TRANSPORTERS];
-    bool tv[MARL_S_TRANSPORTERS];
-    float cur0[MARL_S_TRANSPORTERS], uptakes[MARL_S_TRANSPORTERS];
+    float uptakes[MARL_S_TRANSPORTERS];
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
-        transporter(tpw, i, te[i], tk[i], tv[i]);
-        rates[i] = R.tp(i);
-        cur0[i] = S.x[tk[i] & 15u][tid];
-        const float ev = te[i] < MARL_S_EXT ? S.ext[te[i]][tid] : 0.0f;
-        uptakes[i] = div_rn(rates[i].x * ev, 1.0f + ev);
+        const uint32_t e = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFu;
+        const float ev = e < MARL_S_EXT ? S.ext[e][tid] : 0.0f;
+        uptakes[i] = div_rn(R.tp(i).x * ev, 1.0f + ev);
     }
-    float w[MARL_S_TRANSPORTERS], d[MARL_S_TRANSPORTERS];
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
-        float cur = cur0[i];
-#pragma unroll
-        for (int j = 0; j < i; ++j)
-            if (tv[j] && tk[j] == tk[i]) cur = w[j];  // the latest earlier write of this species
-        const float secretion = ((first >> i) & 1u) ? sec[i] : div_rn(rates[i].y * cur, 1.0f + cur);
-        w[i] = rclamp(cur + (uptakes[i] - secretion) * dt, 0.0f, c.c_max);
-        d[i] = (secretion - uptakes[i]) * dt;
-    }
-#pragma unroll
-    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i)
-        if (tv[i]) S.x[tk[i]][tid] = w[i];
-    // Field deltas, in transporter order per species (cell.rs:237).
-#pragma unroll
-    for (int s = 0; s < MARL_S_EXT; ++s) {
-        float a = 0.0f;
-#pragma unroll
-        for (int i = 0; i < MARL_S_TRANSPORTERS; ++i)
-            if (tv[i] && te[i] == (uint32_t)s) a = a + d[i];
-        del[s] = a;
+        const uint32_t pair = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+        const uint32_t e = pair & 0xFF, k = pair >> 8;
+        if (e >= MARL_S_EXT || k >= MARL_M_INT) continue;
+        const float2 r = R.tp(i);
+        const float xk = S.x[k][tid];
+        const float uptake = uptakes[i];
+        const float secretion = div_rn(r.y * xk, 1.0f + xk);
+        S.x[k][tid] = rclamp(xk + (uptake - secretion) * dt, 0.0f, c.c_max);
+        S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
     }
     S.x[MARL_M_INT - 1][tid] = light;  // cell.rs:243
 }
@@ -383,77 +332,35 @@ __device__ __noinline__ void receptor_activations(const CellConsts& c, const Cel
 
 // Phase 3 of CellState::tick: the reactions, strictly in slot order
 // (cell.rs:246-285), on S.x.  Returns the number of active reactions.
-//
-// Each reaction reads its four operands (substrate, catalyst, cofactor,
-// product) from shared memory one reaction ahead, while the previous reaction
-// computes, and the up to three values that previous reaction writes
-// (cofactor, then substrate, then product: the later write wins) are forwarded
-// into them in registers.  Every store still goes to shared memory in the
-// reference's order, so the state there is exact after the loop; the chain
-// from one reaction to the next carries no shared-memory round trip.
 template <class Scr, class Rules>
 __device__ __forceinline__ int reactions(const CellConsts& c, Scr& S, const Rules& R) {
     const int tid = threadIdx.x;
     const float dt = c.dt;
     const float feps = 1.1920928955078125e-07f;
     int active = 0;
-    uint4 q = R.rx(0);
-    float ls = S.x[q.x & 15u][tid], lc = S.x[(q.x >> 16) & 15u][tid], lf = S.x[(q.x >> 24) & 15u][tid],
-          lp = S.x[(q.x >> 8) & 15u][tid];
-#pragma unroll
+#pragma unroll 4
     for (int r = 0; r < MARL_R_MAX; ++r) {
-        // Operands of reaction r+1, as memory holds them before reaction r writes.
-        uint4 qn = q;
-        float ns = 0.0f, nc = 0.0f, nf = 0.0f, np = 0.0f;
-        if (r + 1 < MARL_R_MAX) {
-            qn = R.rx(r + 1);
-            ns = S.x[qn.x & 15u][tid];
-            nc = S.x[(qn.x >> 16) & 15u][tid];
-            nf = S.x[(qn.x >> 24) & 15u][tid];
-            np = S.x[(qn.x >> 8) & 15u][tid];
-        }
+        const uint4 q = R.rx(r);
         const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF, ci = (q.x >> 16) & 0xFF, fi = q.x >> 24;
         const float km = __uint_as_float(q.y), vmax = __uint_as_float(q.z), kcat = __uint_as_float(q.w);
         if (fabsf(vmax) > c.thr && si != pi) ++active;
-        const bool run = !(fabsf(vmax) < c.thr) && si != pi && si < MARL_M_INT && pi < MARL_M_INT && ci < MARL_M_INT;
-        const bool cof = run && fi != MARL_NO_COFACTOR && fi < MARL_M_INT;
-        float wf = 0.0f, ws = 0.0f, wp = 0.0f;
-        if (run) {
-            const float s = ls;
-            const float cc = lc;
-            const float substrate_term = div_rn(s, km + s + feps);
-            const float catalyst_term = c.epsilon + div_rn(cc, kcat + cc + feps);
-            float rate = vmax * substrate_term * catalyst_term;
-            float xs = s, xp = lp;
-            if (cof) {
-                const float cofv = lf;
-                rate *= div_rn(cofv, 1.0f + cofv);
-                const float consumed = fminf(0.5f * rate * dt, cofv);
-                wf = cofv - consumed;
-                S.x[fi][tid] = wf;
-                if (fi == si) xs = wf;
-                if (fi == pi) xp = wf;
-            }
-            const float flux = fminf(rate * dt, xs);
-            ws = xs - flux;
-            S.x[si][tid] = ws;
-            wp = fminf(xp + flux, c.c_max);
-            S.x[pi][tid] = wp;
+        if (fabsf(vmax) < c.thr) continue;
+        if (si == pi) continue;
+        if (si >= MARL_M_INT || pi >= MARL_M_INT || ci >= MARL_M_INT) continue;
+        const float s = S.x[si][tid];
+        const float cc = S.x[ci][tid];
+        const float substrate_term = div_rn(s, km + s + feps);
+        const float catalyst_term = c.epsilon + div_rn(cc, kcat + cc + feps);
+        float rate = vmax * substrate_term * catalyst_term;
+        if (fi != MARL_NO_COFACTOR && fi < MARL_M_INT) {
+            const float cof = S.x[fi][tid];
+            rate *= div_rn(cof, 1.0f + cof);
+            const float consumed = fminf(0.5f * rate * dt, S.x[fi][tid]);
+            S.x[fi][tid] = S.x[fi][tid] - consumed;
         }
-        if (r + 1 < MARL_R_MAX) {
-            const uint32_t nsi = qn.x & 0xFF, npi = (qn.x >> 8) & 0xFF, nci = (qn.x >> 16) & 0xFF, nfi = qn.x >> 24;
-            auto fwd = [&](float val, uint32_t idx) {
-                if (cof && idx == fi) val = wf;
-                if (run && idx == si) val = ws;
-                if (run && idx == pi) val = wp;
-                return val;
-            };
-            ls = fwd(ns, nsi);
-            lc = fwd(nc, nci);
-            lf = fwd(nf, nfi);
-            lp = fwd(np, npi);
-            q = qn;
-        }
+        const float flux = fminf(rate * dt, S.x[si][tid]);
+        S.x[si][tid] = S.x[si][tid] - flux;
+        S.x[pi][tid] = fminf(S.x[pi][tid] + flux, c.c_max);
     }
     return active;
 }
@@ -493,13 +400,10 @@ __device__ __forceinline__ void surrogate_features(const CellScratch& S, float l
 }
 
 // Maintenance and effectors (phases 3b-4 of CellState::tick, cell.rs:291-329)
-// on the reaction phase's output in S.x; effector secretions are added to
-// del[].  As in transport, every effector's species is read up front and an
-// earlier effector's write of the same species is forwarded in registers.
+// on the reaction phase's output in S.x; effector secretions go to S.del.
 template <class Scr, class Rules>
 __device__ __forceinline__ void maintenance_effectors(const CellConsts& c, Scr& S, const Rules& R, const float4 fate,
-                                                      uint32_t prep, uint32_t quiescent, int active,
-                                                      float (&del)[MARL_S_EXT]) {
+                                                      uint32_t prep, uint32_t quiescent, int active) {
     const int tid = threadIdx.x;
     const float dt = c.dt;
     // Maintenance (cell.rs:291-311)
@@ -520,50 +424,27 @@ __device__ __forceinline__ void maintenance_effectors(const CellConsts& c, Scr& 
     if (!quiescent) {
         const uint4 efi = R.ef_idx();
         const uint32_t efw[4] = {efi.x, efi.y, efi.z, efi.w};
-        uint32_t ek[MARL_S_EFFECTORS], ee[MARL_S_EFFECTORS];
-        bool ev[MARL_S_EFFECTORS], fired[MARL_S_EFFECTORS];
-        float2 par[MARL_S_EFFECTORS];
-        float cur0[MARL_S_EFFECTORS], w[MARL_S_EFFECTORS], amount[MARL_S_EFFECTORS];
 #pragma unroll
         for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
-            const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;  // int | ext << 8
-            ek[i] = pair & 0xFF;
-            ee[i] = pair >> 8;
-            ev[i] = ek[i] < MARL_M_INT && ee[i] < MARL_S_EXT;
-            par[i] = R.ef(i);
-            cur0[i] = S.x[ek[i] & 15u][tid];
-        }
-#pragma unroll
-        for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
-            float cur = cur0[i];
-#pragma unroll
-            for (int j = 0; j < i; ++j)
-                if (fired[j] && ek[j] == ek[i]) cur = w[j];
-            fired[i] = ev[i] && cur > par[i].x;
-            amount[i] = 0.0f;
-            w[i] = cur;
-            if (fired[i]) {
-                amount[i] = div_rn(par[i].y * cur, 1.0f + cur) * dt;
-                w[i] = fmaxf(cur - amount[i], 0.0f);
+            const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+            const uint32_t k = pair & 0xFF, e = pair >> 8;
+            if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
+            const float2 pr = R.ef(i);
+            const float xk = S.x[k][tid];
+            if (xk > pr.x) {
+                const float amount = div_rn(pr.y * xk, 1.0f + xk) * dt;
+                S.x[k][tid] = fmaxf(xk - amount, 0.0f);
+                S.del[e][tid] = S.del[e][tid] + amount;
             }
-        }
-#pragma unroll
-        for (int i = 0; i < MARL_S_EFFECTORS; ++i)
-            if (fired[i]) S.x[ek[i]][tid] = w[i];
-#pragma unroll
-        for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
-#pragma unroll
-            for (int s = 0; s < MARL_S_EXT; ++s)
-                if (fired[i] && ee[i] == (uint32_t)s) del[s] = del[s] + amount[i];
         }
     }
 }
 
-template <bool LEAN>
-using ScratchOf = typename std::conditional<LEAN, LeanScratch, CellScratch>::type;
-template <bool LEAN>
-using RulesOf = typename std::conditional<LEAN, TableRules, StagedRules>::type;
-
+// Gather -> tick -> scatter of cell j, after all its dependencies are done.
+// MODE: kModePlain, kModeCapture (also writes the cell's surrogate training
+// row), kModeGated / kModeTrusted (reaction phase from the surrogate where
+// the pre-pass speculation holds; see SurrView).  LEAN: the throughput form
+// (TableRules, LeanScratch), plain mode only.
 template <bool LEAN>
 __device__ __forceinline__ RulesOf<LEAN> rules_of(const ScratchOf<LEAN>& S, const CellTable& t, uint32_t j) {
     if constexpr (LEAN)
@@ -572,14 +453,9 @@ __device__ __forceinline__ RulesOf<LEAN> rules_of(const ScratchOf<LEAN>& S, cons
         return StagedRules{S};
 }
 
-// Gather -> tick -> scatter of cell j, after all its dependencies are done.
-// MODE: kModePlain, kModeCapture (also writes the cell's surrogate training
-// row), kModeGated / kModeTrusted (reaction phase from the surrogate where
-// the pre-pass speculation holds; see SurrView).  LEAN: the throughput form
-// (TableRules, LeanScratch), plain mode only.
 template <int MODE, bool LEAN = false>
 __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf<LEAN>& S, uint32_t j,
-                            const CellPre& pre, const float (&sec)[MARL_S_TRANSPORTERS], uint32_t first) {
+                            const CellPre& pre) {
     static_assert(!LEAN || MODE == kModePlain, "the throughput form is the plain tick");
     const int tid = threadIdx.x;
     const CellTable& t = *v.t;
@@ -595,18 +471,17 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
     const uint32_t st = pre.state;
     uint32_t prep = st & 0xFFFFu;
     uint32_t quiescent = (st >> 16) & 1u;
+    const float4 fate = R.fate();
 
     // The gathered neighbour values are also the scatter's starting values:
     // no other cell touches N(j) while this cell holds it.  (The throughput
     // form reads them again for the scatter instead of holding them.)
     float4 nv[6][3];
-    float del[MARL_S_EXT];
-    gather_transport(v, c, S, R, pre, sec, first, nv, del);
+    gather_transport(v, c, S, R, pre, nv);
     if (v.act) receptor_activations(c, t, j, S, v.act);
 
     int active;
     bool finished = false;  // maintenance and effectors already applied
-    const float4 fate = R.fate();
     if constexpr (MODE == kModePlain) {
         active = reactions(c, S, R);
     } else if constexpr (MODE == kModeCapture) {
@@ -645,8 +520,8 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
                 // the 16 species).  Its effector secretions go with it.
                 float del_t[MARL_S_EXT], xp[MARL_M_INT], dp[MARL_S_EXT];
 #pragma unroll
-                for (int e = 0; e < MARL_S_EXT; ++e) del_t[e] = del[e];
-                maintenance_effectors(c, S, R, fate, prep, quiescent, active, del);
+                for (int e = 0; e < MARL_S_EXT; ++e) del_t[e] = S.del[e][tid];
+                maintenance_effectors(c, S, R, fate, prep, quiescent, active);
 #pragma unroll
                 for (int k = 0; k < MARL_M_INT; ++k) {
                     xp[k] = S.x[k][tid];
@@ -654,10 +529,10 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
                 }
 #pragma unroll
                 for (int e = 0; e < MARL_S_EXT; ++e) {
-                    dp[e] = del[e];
-                    del[e] = del_t[e];
+                    dp[e] = S.del[e][tid];
+                    S.del[e][tid] = del_t[e];
                 }
-                maintenance_effectors(c, S, R, fate, prep, quiescent, active, del);
+                maintenance_effectors(c, S, R, fate, prep, quiescent, active);
                 float num = 0.0f, den = 0.0f;
 #pragma unroll
                 for (int k = 0; k < MARL_M_INT; ++k) {
@@ -671,7 +546,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
 #pragma unroll
                     for (int k = 0; k < MARL_M_INT; ++k) S.x[k][tid] = xp[k];
 #pragma unroll
-                    for (int e = 0; e < MARL_S_EXT; ++e) del[e] = dp[e];
+                    for (int e = 0; e < MARL_S_EXT; ++e) S.del[e][tid] = dp[e];
                     status = kSurrRejected;
                 }
                 finished = true;
@@ -680,7 +555,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
         sv.status[row] = status;
         sv.err[row] = err;
     }
-    if (!finished) maintenance_effectors(c, S, R, fate, prep, quiescent, active, del);
+    if (!finished) maintenance_effectors(c, S, R, fate, prep, quiescent, active);
 
     // Phase 5: fate (cell.rs:332-366)
     const float energy = S.x[0][tid];
@@ -717,11 +592,11 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
         if (n == 1 || n == 2 || n == 4) {
             const float inv = n == 1 ? 1.0f : (n == 2 ? 0.5f : 0.25f);
 #pragma unroll
-            for (int s = 0; s < 12; ++s) split[s] = del[s] * inv;
+            for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] * inv;
         } else {
             const float nf = (float)n;
 #pragma unroll
-            for (int s = 0; s < 12; ++s) split[s] = div_rn(del[s], nf);
+            for (int s = 0; s < 12; ++s) split[s] = div_rn(S.del[s][tid], nf);
         }
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
@@ -763,13 +638,9 @@ __device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellCon
         CellRunView v{};
         uint32_t j = 0;
         CellPre pre;
-        float sec[MARL_S_TRANSPORTERS];
-        uint32_t first = 0;
         if (pending) {
             resolve(gi, v, j);
             stage_cell(v, S, j, pre);
-            cp_async_wait_all();  // the staged state, for the secretions computed during the wait
-            presecretions(S, rules_of<LEAN>(S, *v.t, j), sec, first);
         }
         // Dependencies not yet seen finished (bit f: face f).  A poll loads
         // them with relaxed loads, all in flight together; once every one has
@@ -789,7 +660,7 @@ __device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellCon
                     if (((remaining >> f) & 1u) && seen[f] == v.epoch) remaining &= ~(1u << f);
                 if (remaining == 0) {
                     fence_acquire_gpu();
-                    update_cell<MODE, LEAN>(v, c, S, j, pre, sec, first);
+                    update_cell<MODE, LEAN>(v, c, S, j, pre);
                     // release: this cell's field writes are visible before its done flag
                     st_release_u32(&t.done[j], v.epoch);
                     pending = false;
@@ -800,6 +671,7 @@ __device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellCon
                     if (pending) {
                         const CellTable& t = *v.t;
                         atomicOr(err, kErrTimeoutDeps);
+                        cp_async_wait_all();  // drain this lane's staging copies
                         t.events[j] = MARL_EVENT_NONE;
                         st_release_u32(&t.done[j], v.epoch);
                         pending = false;
@@ -813,7 +685,7 @@ __device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellCon
 }
 
 template <int MODE, bool LEAN>
-__global__ void __launch_bounds__(kTickThreads, LEAN ? 4 : 3) k_cell_tick(const __grid_constant__ CellLaunch a) {
+__global__ void __launch_bounds__(kTickThreads, LEAN ? 5 : 3) k_cell_tick(const __grid_constant__ CellLaunch a) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     ScratchOf<LEAN>& S = *reinterpret_cast<ScratchOf<LEAN>*>(tick_smem);
     const uint32_t total = a.n_dev ? *a.n_dev : a.n;
@@ -831,14 +703,8 @@ __device__ __forceinline__ void prepass_cell(const CellRunView& v, const CellCon
                                              float* __restrict__ xt, __nv_bfloat16* __restrict__ X) {
     CellPre pre;
     stage_cell(v, S, j, pre);
-    cp_async_wait_all();
-    const StagedRules R{S};
-    float sec[MARL_S_TRANSPORTERS];
-    uint32_t first = 0;
-    presecretions(S, R, sec, first);
     float4 nv[6][3];
-    float del[MARL_S_EXT];
-    gather_transport(v, c, S, R, pre, sec, first, nv, del);
+    gather_transport(v, c, S, StagedRules{S}, pre, nv);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) xt[k * ld + row] = S.x[k][threadIdx.x];
     float f[mlp::kInPad];
@@ -927,7 +793,7 @@ __global__ void k_surrogate_count(const uint8_t* __restrict__ status, const floa
 // cell j is ticket cell_base(r) + j), so every dependency of a cell, which lies
 // in the same run at a smaller index, also has a smaller ticket.
 template <int MODE>
-__global__ void __launch_bounds__(kTickThreads, 3) k_cell_tick_batch(const RunDesc* __restrict__ runs, int n_runs,
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc* __restrict__ runs, int n_runs,
                                                                   BatchScalars* __restrict__ bs, CellConsts c,
                                                                   int parity) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
