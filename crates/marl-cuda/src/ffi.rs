@@ -36,10 +36,6 @@ pub const MARL_EVENT_QUIESCENCE: u8 = 3;
 pub const MARL_SOURCES_ADDITIVE: u32 = 0;
 pub const MARL_SOURCES_DIRICHLET: u32 = 1;
 
-pub const MARL_CELL_FORM_AUTO: i32 = 0;
-pub const MARL_CELL_FORM_LATENCY: i32 = 1;
-pub const MARL_CELL_FORM_THROUGHPUT: i32 = 2;
-
 pub const MARL_RULESETS_LAYERS: i32 = 1;
 pub const MARL_RULESETS_FULL: i32 = 2;
 pub const MARL_RULESETS_BOTH: i32 = 3;
@@ -334,7 +330,6 @@ unsafe extern "C" {
     pub fn marl_ctx_set_tile(ctx: *mut Ctx, tile: i32, zc: i32) -> Status;
     pub fn marl_ctx_get_tile(ctx: *mut Ctx, tile: *mut i32, zc: *mut i32) -> Status;
     pub fn marl_ctx_set_cell_lanes(ctx: *mut Ctx, lanes: u32) -> Status;
-    pub fn marl_ctx_set_cell_form(ctx: *mut Ctx, form: i32) -> Status;
     pub fn marl_ctx_set_wait_limit(ctx: *mut Ctx, polls: u32) -> Status;
     pub fn marl_ctx_test_hold_dependency(ctx: *mut Ctx, cell: u32, face: u32, slot: u32) -> Status;
     pub fn marl_ctx_set_receptor_output(ctx: *mut Ctx, enable: i32) -> Status;

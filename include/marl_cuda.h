@@ -243,18 +243,6 @@ marl_status marl_ctx_get_tile(marl_ctx* ctx, int32_t* tile, int32_t* zc);
  * per warp serialise less work inside a warp along the dependency chains, at
  * the cost of more warps.  Results do not depend on it. */
 marl_status marl_ctx_set_cell_lanes(marl_ctx* ctx, uint32_t lanes);
-/* Form of the plain cell loop (no reference counterpart; results do not
- * depend on it).  LATENCY stages each cell's ruleset into shared memory while
- * the cell waits for its dependencies and keeps the gathered neighbour values
- * in registers for the scatter: the shortest update, for colonies whose cells
- * wait on long dependency chains.  THROUGHPUT reads the ruleset where it is
- * used and reads the neighbours again for the scatter, so the kernel needs
- * far less shared memory and fewer registers and more warps fit on an SM:
- * for large populations of mostly independent cells.  AUTO (the default)
- * takes THROUGHPUT from 131,072 cells.  The surrogate modes always use the
- * latency form. */
-enum { MARL_CELL_FORM_AUTO = 0, MARL_CELL_FORM_LATENCY = 1, MARL_CELL_FORM_THROUGHPUT = 2 };
-marl_status marl_ctx_set_cell_form(marl_ctx* ctx, int32_t form);
 /* Bound of the cell loop's dependency waits (no reference counterpart; the
  * reference loop is sequential and never waits).  A cell that has polled an
  * unfinished dependency `polls` times gives up: it is left un-updated with

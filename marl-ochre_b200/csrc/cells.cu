@@ -24,8 +24,6 @@
 
 #include <cuda_bf16.h>
 
-#include <type_traits>
-
 #include "common.cuh"
 #include "internal.h"
 #include "kernel_setup.h"
@@ -113,47 +111,6 @@ struct CellScratch {
 };
 constexpr int kTickSmem = (int)sizeof(CellScratch);
 
-// Per-thread state of the throughput form: only what is indexed dynamically
-// (the internal species, the gathered environment and the field deltas).
-struct LeanScratch {
-    float x[MARL_M_INT][kTickThreads];
-    float ext[MARL_S_EXT][kTickThreads];
-    float del[MARL_S_EXT][kTickThreads];
-};
-constexpr int kTickSmemLean = (int)sizeof(LeanScratch);
-
-// The cell's ruleset as the update reads it.  StagedRules: copied into shared
-// memory while the cell waits for its dependencies (the latency form, for
-// colonies whose cells wait on long dependency chains).  TableRules: read from
-// the table where it is used, through the read-only path (the throughput form,
-// for large populations of mostly independent cells: 20 KB of shared memory
-// per 128 threads instead of 75.8 KB, and the gathered neighbour values are
-// read again for the scatter instead of held in registers, so more warps fit
-// on an SM).  Both give the same bits: only where the values come from differs.
-struct StagedRules {
-    const CellScratch& S;
-    __device__ __forceinline__ uint4 rx(int r) const { return S.rx[r][threadIdx.x]; }
-    __device__ __forceinline__ float2 tp(int i) const { return S.tp[i][threadIdx.x]; }
-    __device__ __forceinline__ float2 ef(int i) const { return S.ef[i][threadIdx.x]; }
-    __device__ __forceinline__ uint4 tp_idx() const { return S.idx[0][threadIdx.x]; }
-    __device__ __forceinline__ uint4 ef_idx() const { return S.idx[1][threadIdx.x]; }
-    __device__ __forceinline__ float4 fate() const { return S.fate[threadIdx.x]; }
-};
-struct TableRules {
-    const CellTable& t;
-    uint32_t j;
-    __device__ __forceinline__ uint4 rx(int r) const { return __ldg(&t.rx[(size_t)r * t.cap + j]); }
-    __device__ __forceinline__ float2 tp(int i) const { return __ldg(&t.tp_rate[(size_t)i * t.cap + j]); }
-    __device__ __forceinline__ float2 ef(int i) const { return __ldg(&t.ef_par[(size_t)i * t.cap + j]); }
-    __device__ __forceinline__ uint4 tp_idx() const { return __ldg(&t.tp_idx[j]); }
-    __device__ __forceinline__ uint4 ef_idx() const { return __ldg(&t.ef_idx[j]); }
-    __device__ __forceinline__ float4 fate() const { return __ldg(&t.fate[j]); }
-};
-template <bool LEAN>
-using ScratchOf = typename std::conditional<LEAN, LeanScratch, CellScratch>::type;
-template <bool LEAN>
-using RulesOf = typename std::conditional<LEAN, TableRules, StagedRules>::type;
-
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -179,7 +136,7 @@ __device__ __forceinline__ float rclamp(float v, float lo, float hi) {  // Rust 
 // Everything a cell's update needs that no other cell of this tick writes:
 // staged before the cell waits on its dependencies.
 struct CellPre {
-    uint32_t nb, pos, state;
+    uint32_t nb, pos, state, age;
     float light;
     int32_t dep[6];
 };
@@ -195,30 +152,26 @@ struct CellRunView {
     float* act;          // receptor activations [8][cap], or null
 };
 
-// Staging before the dependency wait: the internal state (and, in the latency
-// form, the ruleset) by asynchronous copies into shared memory, and the
-// per-cell scalars.
-template <class Scr>
-__device__ __forceinline__ void stage_cell(const CellRunView& v, Scr& S, uint32_t j, CellPre& pre) {
+__device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j, CellPre& pre) {
     const int tid = threadIdx.x;
     const CellTable& t = *v.t;
     const size_t cap = t.cap;
-    if constexpr (std::is_same<Scr, CellScratch>::value) {
+    // Ruleset and internal state: asynchronous copies into shared memory.
 #pragma unroll
-        for (int r = 0; r < MARL_R_MAX; ++r) cp_async16(&S.rx[r][tid], &t.rx[r * cap + j]);
+    for (int r = 0; r < MARL_R_MAX; ++r) cp_async16(&S.rx[r][tid], &t.rx[r * cap + j]);
 #pragma unroll
-        for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) cp_async8(&S.tp[i][tid], &t.tp_rate[i * cap + j]);
+    for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) cp_async8(&S.tp[i][tid], &t.tp_rate[i * cap + j]);
 #pragma unroll
-        for (int i = 0; i < MARL_S_EFFECTORS; ++i) cp_async8(&S.ef[i][tid], &t.ef_par[i * cap + j]);
-        cp_async16(&S.idx[0][tid], &t.tp_idx[j]);
-        cp_async16(&S.idx[1][tid], &t.ef_idx[j]);
-        cp_async16(&S.fate[tid], &t.fate[j]);
-    }
+    for (int i = 0; i < MARL_S_EFFECTORS; ++i) cp_async8(&S.ef[i][tid], &t.ef_par[i * cap + j]);
+    cp_async16(&S.idx[0][tid], &t.tp_idx[j]);
+    cp_async16(&S.idx[1][tid], &t.ef_idx[j]);
+    cp_async16(&S.fate[tid], &t.fate[j]);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) cp_async4(&S.x[k][tid], &t.internal[k * cap + j]);
     pre.nb = t.nb[j];
     pre.pos = t.pos[j];
     pre.state = t.state[j];
+    pre.age = t.age[j];
 #pragma unroll
     for (int f = 0; f < 6; ++f) pre.dep[f] = ((pre.nb >> f) & 1u) ? t.dep[(size_t)f * cap + j] : -1;
     const Grid g = v.g;
@@ -230,8 +183,7 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, Scr& S, uint32_
 // S.x the internal state after transport with the light in slot 15.  Shared
 // by the cell loop and the surrogate's pre-pass, so both produce the same bits
 // from the same field.
-template <class Scr, class Rules>
-__device__ __forceinline__ void gather_transport(const CellRunView& v, const CellConsts& c, Scr& S, const Rules& R,
+__device__ __forceinline__ void gather_transport(const CellRunView& v, const CellConsts& c, CellScratch& S,
                                                  const CellPre& pre, float4 (&nv)[6][3]) {
     const int tid = threadIdx.x;
     const Grid g = v.g;
@@ -282,21 +234,21 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
     // Phase 2: transport (cell.rs:223-238).  Uptake depends only on the
     // gathered environment, so all eight are evaluated first; secretion
     // follows the internal state transporter by transporter.
-    const uint4 tpi = R.tp_idx();
+    const uint4 tpi = S.idx[0][tid];
     const uint32_t tpw[4] = {tpi.x, tpi.y, tpi.z, tpi.w};
     float uptakes[MARL_S_TRANSPORTERS];
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
         const uint32_t e = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFu;
         const float ev = e < MARL_S_EXT ? S.ext[e][tid] : 0.0f;
-        uptakes[i] = div_rn(R.tp(i).x * ev, 1.0f + ev);
+        uptakes[i] = div_rn(S.tp[i][tid].x * ev, 1.0f + ev);
     }
 #pragma unroll
     for (int i = 0; i < MARL_S_TRANSPORTERS; ++i) {
         const uint32_t pair = (tpw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
         const uint32_t e = pair & 0xFF, k = pair >> 8;
         if (e >= MARL_S_EXT || k >= MARL_M_INT) continue;
-        const float2 r = R.tp(i);
+        const float2 r = S.tp[i][tid];
         const float xk = S.x[k][tid];
         const float uptake = uptakes[i];
         const float secretion = div_rn(r.y * xk, 1.0f + xk);
@@ -310,9 +262,8 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
 // from gathered species i, into act[i][j].  The reference computes it into an
 // unused local; here it is an optional output.  Not inlined, so that the
 // update's register allocation does not carry it when the output is off.
-template <class Scr>
-__device__ __noinline__ void receptor_activations(const CellConsts& c, const CellTable& t, uint32_t j, const Scr& S,
-                                                  float* act) {
+__device__ __noinline__ void receptor_activations(const CellConsts& c, const CellTable& t, uint32_t j,
+                                                  const CellScratch& S, float* act) {
     const float* r = t.cold + (size_t)j * kColdFloats;  // receptors: k_half, n_hill, gain
 #pragma unroll 1
     for (int i = 0; i < MARL_S_RECEPTORS; ++i) {
@@ -332,15 +283,14 @@ __device__ __noinline__ void receptor_activations(const CellConsts& c, const Cel
 
 // Phase 3 of CellState::tick: the reactions, strictly in slot order
 // (cell.rs:246-285), on S.x.  Returns the number of active reactions.
-template <class Scr, class Rules>
-__device__ __forceinline__ int reactions(const CellConsts& c, Scr& S, const Rules& R) {
+__device__ __forceinline__ int reactions(const CellConsts& c, CellScratch& S) {
     const int tid = threadIdx.x;
     const float dt = c.dt;
     const float feps = 1.1920928955078125e-07f;
     int active = 0;
 #pragma unroll 4
     for (int r = 0; r < MARL_R_MAX; ++r) {
-        const uint4 q = R.rx(r);
+        const uint4 q = S.rx[r][tid];
         const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF, ci = (q.x >> 16) & 0xFF, fi = q.x >> 24;
         const float km = __uint_as_float(q.y), vmax = __uint_as_float(q.z), kcat = __uint_as_float(q.w);
         if (fabsf(vmax) > c.thr && si != pi) ++active;
@@ -367,12 +317,11 @@ __device__ __forceinline__ int reactions(const CellConsts& c, Scr& S, const Rule
 
 // Active-reaction count alone (the maintenance term of cell.rs:291-311),
 // for cells whose reaction phase the surrogate replaces.
-template <class Rules>
-__device__ __forceinline__ int active_reactions(const CellConsts& c, const Rules& R) {
+__device__ __forceinline__ int active_reactions(const CellConsts& c, const CellScratch& S) {
     int active = 0;
 #pragma unroll
     for (int r = 0; r < MARL_R_MAX; ++r) {
-        const uint4 q = R.rx(r);
+        const uint4 q = S.rx[r][threadIdx.x];
         const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF;
         if (fabsf(__uint_as_float(q.z)) > c.thr && si != pi) ++active;
     }
@@ -401,8 +350,7 @@ __device__ __forceinline__ void surrogate_features(const CellScratch& S, float l
 
 // Maintenance and effectors (phases 3b-4 of CellState::tick, cell.rs:291-329)
 // on the reaction phase's output in S.x; effector secretions go to S.del.
-template <class Scr, class Rules>
-__device__ __forceinline__ void maintenance_effectors(const CellConsts& c, Scr& S, const Rules& R, const float4 fate,
+__device__ __forceinline__ void maintenance_effectors(const CellConsts& c, CellScratch& S, const float4 fate,
                                                       uint32_t prep, uint32_t quiescent, int active) {
     const int tid = threadIdx.x;
     const float dt = c.dt;
@@ -422,14 +370,14 @@ __device__ __forceinline__ void maintenance_effectors(const CellConsts& c, Scr& 
 
     // Effectors (cell.rs:314-329)
     if (!quiescent) {
-        const uint4 efi = R.ef_idx();
+        const uint4 efi = S.idx[1][tid];
         const uint32_t efw[4] = {efi.x, efi.y, efi.z, efi.w};
 #pragma unroll
         for (int i = 0; i < MARL_S_EFFECTORS; ++i) {
             const uint32_t pair = (efw[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
             const uint32_t k = pair & 0xFF, e = pair >> 8;
             if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
-            const float2 pr = R.ef(i);
+            const float2 pr = S.ef[i][tid];
             const float xk = S.x[k][tid];
             if (xk > pr.x) {
                 const float amount = div_rn(pr.y * xk, 1.0f + xk) * dt;
@@ -443,23 +391,12 @@ __device__ __forceinline__ void maintenance_effectors(const CellConsts& c, Scr& 
 // Gather -> tick -> scatter of cell j, after all its dependencies are done.
 // MODE: kModePlain, kModeCapture (also writes the cell's surrogate training
 // row), kModeGated / kModeTrusted (reaction phase from the surrogate where
-// the pre-pass speculation holds; see SurrView).  LEAN: the throughput form
-// (TableRules, LeanScratch), plain mode only.
-template <bool LEAN>
-__device__ __forceinline__ RulesOf<LEAN> rules_of(const ScratchOf<LEAN>& S, const CellTable& t, uint32_t j) {
-    if constexpr (LEAN)
-        return TableRules{t, j};
-    else
-        return StagedRules{S};
-}
-
-template <int MODE, bool LEAN = false>
-__device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf<LEAN>& S, uint32_t j,
+// the pre-pass speculation holds; see SurrView).
+template <int MODE>
+__device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
                             const CellPre& pre) {
-    static_assert(!LEAN || MODE == kModePlain, "the throughput form is the plain tick");
     const int tid = threadIdx.x;
     const CellTable& t = *v.t;
-    const auto R = rules_of<LEAN>(S, t, j);
     const Grid g = v.g;
     const uint32_t nb = pre.nb;
     const uint32_t P = pre.pos;
@@ -471,25 +408,24 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
     const uint32_t st = pre.state;
     uint32_t prep = st & 0xFFFFu;
     uint32_t quiescent = (st >> 16) & 1u;
-    const float4 fate = R.fate();
+    const float4 fate = S.fate[tid];
 
     // The gathered neighbour values are also the scatter's starting values:
-    // no other cell touches N(j) while this cell holds it.  (The throughput
-    // form reads them again for the scatter instead of holding them.)
+    // no other cell touches N(j) while this cell holds it.
     float4 nv[6][3];
-    gather_transport(v, c, S, R, pre, nv);
+    gather_transport(v, c, S, pre, nv);
     if (v.act) receptor_activations(c, t, j, S, v.act);
 
     int active;
     bool finished = false;  // maintenance and effectors already applied
     if constexpr (MODE == kModePlain) {
-        active = reactions(c, S, R);
+        active = reactions(c, S);
     } else if constexpr (MODE == kModeCapture) {
         const SurrView& sv = *v.sv;
         const bool cap_row = j < sv.raw_rows;
         float* row = sv.raw + (size_t)j * MARL_SURR_RAW_STRIDE;
         if (cap_row) surrogate_features(S, pre.light, [&](int f, float val) { row[f] = val; });
-        active = reactions(c, S, R);
+        active = reactions(c, S);
         if (cap_row) {
 #pragma unroll
             for (int k = 0; k < MARL_M_INT; ++k) row[MARL_SURR_FEATURES + k] = S.x[k][tid] - row[k];
@@ -505,13 +441,13 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
         uint8_t status = kSurrNotSpeculated;
         float err = 0.0f;
         if (MODE == kModeTrusted && spec) {
-            active = active_reactions(c, R);
+            active = active_reactions(c, S);
 #pragma unroll
             for (int k = 0; k < MARL_M_INT; ++k)
                 S.x[k][tid] = fminf(fmaxf(S.x[k][tid] + sv.pred[k * ld + row], 0.0f), c.c_max);
             status = kSurrAccepted;
         } else {
-            active = reactions(c, S, R);
+            active = reactions(c, S);
             if (MODE == kModeGated && spec) {
                 // The plain kernel judges the state the cell keeps: maintenance
                 // and effectors run on the plain reaction output and on the
@@ -521,7 +457,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
                 float del_t[MARL_S_EXT], xp[MARL_M_INT], dp[MARL_S_EXT];
 #pragma unroll
                 for (int e = 0; e < MARL_S_EXT; ++e) del_t[e] = S.del[e][tid];
-                maintenance_effectors(c, S, R, fate, prep, quiescent, active);
+                maintenance_effectors(c, S, fate, prep, quiescent, active);
 #pragma unroll
                 for (int k = 0; k < MARL_M_INT; ++k) {
                     xp[k] = S.x[k][tid];
@@ -532,7 +468,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
                     dp[e] = S.del[e][tid];
                     S.del[e][tid] = del_t[e];
                 }
-                maintenance_effectors(c, S, R, fate, prep, quiescent, active);
+                maintenance_effectors(c, S, fate, prep, quiescent, active);
                 float num = 0.0f, den = 0.0f;
 #pragma unroll
                 for (int k = 0; k < MARL_M_INT; ++k) {
@@ -555,11 +491,10 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
         sv.status[row] = status;
         sv.err[row] = err;
     }
-    if (!finished) maintenance_effectors(c, S, R, fate, prep, quiescent, active);
+    if (!finished) maintenance_effectors(c, S, fate, prep, quiescent, active);
 
     // Phase 5: fate (cell.rs:332-366)
     const float energy = S.x[0][tid];
-    t.age[j] = t.age[j] + 1;
     const float eff_death = fmaxf(fate.y, c.hard_death_floor);
     uint8_t event;
     if (energy < eff_death) {
@@ -580,10 +515,6 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
         quiescent = 0;
         event = MARL_EVENT_NONE;
     }
-    t.state[j] = (st & 0xFF000000u) | (quiescent << 16) | prep;
-    t.events[j] = event;
-#pragma unroll
-    for (int k = 0; k < MARL_M_INT; ++k) t.internal[(size_t)k * t.cap + j] = S.x[k][tid];
 
     // Scatter: split deltas over the same neighbours, clamp after each add
     // (spatial.rs:87-110, field.rs:57-62).
@@ -602,12 +533,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
         for (int f = 0; f < 6; ++f) {
             if (!((nb >> f) & 1u)) continue;
             float* dst = v.field + (size_t)((long long)vox + off[f]) * 12;
-            float4 q0, q1, q2;
-            if constexpr (LEAN) {
-                q0 = ld4(dst), q1 = ld4(dst + 4), q2 = ld4(dst + 8);
-            } else {
-                q0 = nv[f][0], q1 = nv[f][1], q2 = nv[f][2];
-            }
+            float4 q0 = nv[f][0], q1 = nv[f][1], q2 = nv[f][2];
             q0 = make_float4(fmaxf(q0.x + split[0], 0.0f), fmaxf(q0.y + split[1], 0.0f), fmaxf(q0.z + split[2], 0.0f),
                              fmaxf(q0.w + split[3], 0.0f));
             q1 = make_float4(fmaxf(q1.x + split[4], 0.0f), fmaxf(q1.y + split[5], 0.0f), fmaxf(q1.z + split[6], 0.0f),
@@ -619,13 +545,21 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, ScratchOf
             st4(dst + 8, q2);
         }
     }
+    // Publish: the scatter's writes are visible before the done flag (release).
+    // Only later kernels read the cell's own state, so it is stored after.
+    st_release_u32(&t.done[j], v.epoch);
+    t.age[j] = pre.age + 1;
+    t.state[j] = (st & 0xFF000000u) | (quiescent << 16) | prep;
+    t.events[j] = event;
+#pragma unroll
+    for (int k = 0; k < MARL_M_INT; ++k) t.internal[(size_t)k * t.cap + j] = S.x[k][tid];
 }
 
 // The ticket loop shared by the single-run and the batched kernel.  `resolve`
 // maps a ticket (global cell index) to the lane's run view and local index.
-template <int MODE, bool LEAN, class Resolve>
-__device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellConsts& c, uint32_t total,
-                                               uint32_t* ticket, uint32_t* err, uint32_t lanes, Resolve resolve) {
+template <int MODE, class Resolve>
+__device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts& c, uint32_t total, uint32_t* ticket,
+                                               uint32_t* err, uint32_t lanes, Resolve resolve) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -660,9 +594,7 @@ __device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellCon
                     if (((remaining >> f) & 1u) && seen[f] == v.epoch) remaining &= ~(1u << f);
                 if (remaining == 0) {
                     fence_acquire_gpu();
-                    update_cell<MODE, LEAN>(v, c, S, j, pre);
-                    // release: this cell's field writes are visible before its done flag
-                    st_release_u32(&t.done[j], v.epoch);
+                    update_cell<MODE>(v, c, S, j, pre);  // publishes done[j] itself
                     pending = false;
                 }
             }
@@ -684,12 +616,12 @@ __device__ __forceinline__ void cell_tick_loop(ScratchOf<LEAN>& S, const CellCon
     }
 }
 
-template <int MODE, bool LEAN>
-__global__ void __launch_bounds__(kTickThreads, LEAN ? 5 : 3) k_cell_tick(const __grid_constant__ CellLaunch a) {
+template <int MODE>
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constant__ CellLaunch a) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
-    ScratchOf<LEAN>& S = *reinterpret_cast<ScratchOf<LEAN>*>(tick_smem);
+    CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const uint32_t total = a.n_dev ? *a.n_dev : a.n;
-    cell_tick_loop<MODE, LEAN>(S, a.k, total, a.ticket, a.err, a.lanes, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    cell_tick_loop<MODE>(S, a.k, total, a.ticket, a.err, a.lanes, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv, a.act};
         j = gi;
     });
@@ -704,7 +636,7 @@ __device__ __forceinline__ void prepass_cell(const CellRunView& v, const CellCon
     CellPre pre;
     stage_cell(v, S, j, pre);
     float4 nv[6][3];
-    gather_transport(v, c, S, StagedRules{S}, pre, nv);
+    gather_transport(v, c, S, pre, nv);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) xt[k * ld + row] = S.x[k][threadIdx.x];
     float f[mlp::kInPad];
@@ -798,7 +730,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc*
                                                                   int parity) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
-    cell_tick_loop<MODE, false>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, 32u, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
+    cell_tick_loop<MODE>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, 32u, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         const RunDesc& R = runs[find_run(runs, n_runs, gi)];
         v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv, nullptr};
         j = gi - R.cell_base;
@@ -1170,16 +1102,14 @@ cudaError_t launch_hold_dependency(const CellTable& t, uint32_t cell, int face, 
     return cudaGetLastError();
 }
 
-template <int MODE, bool LEAN = false>
+template <int MODE>
 static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaStream_t s) {
-    constexpr int smem = LEAN ? kTickSmemLean : kTickSmem;
     static std::atomic<int> setup[kSetupDevices];
     int per_sm = 1;
     cudaError_t e = setup_once(setup, &per_sm, [](int* v) {
-        cudaError_t r =
-            cudaFuncSetAttribute(k_cell_tick<MODE, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t r = cudaFuncSetAttribute(k_cell_tick<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
         if (r != cudaSuccess) return r;
-        r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick<MODE, LEAN>, kTickThreads, smem);
+        r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick<MODE>, kTickThreads, kTickSmem);
         if (*v < 1) *v = 1;
         return r;
     });
@@ -1190,16 +1120,14 @@ static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaS
     // ticket holder is running (the dependency waits rely on it).
     const uint32_t resident = (uint32_t)per_sm * (uint32_t)num_sms;
     const uint32_t blocks = blocks_needed < resident ? blocks_needed : resident;
-    k_cell_tick<MODE, LEAN><<<blocks, kTickThreads, smem, s>>>(a);
+    k_cell_tick<MODE><<<blocks, kTickThreads, kTickSmem, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
     switch (a.mode) {
-        case kModePlain:
-            return a.lean ? launch_cell_tick_mode<kModePlain, true>(a, num_sms, s)
-                          : launch_cell_tick_mode<kModePlain>(a, num_sms, s);
+        case kModePlain: return launch_cell_tick_mode<kModePlain>(a, num_sms, s);
         case kModeCapture: return launch_cell_tick_mode<kModeCapture>(a, num_sms, s);
         case kModeGated: return launch_cell_tick_mode<kModeGated>(a, num_sms, s);
         case kModeTrusted: return launch_cell_tick_mode<kModeTrusted>(a, num_sms, s);

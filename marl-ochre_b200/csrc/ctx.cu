@@ -219,10 +219,6 @@ CellLaunch cell_launch(marl_ctx* c) {
     a.lanes = c->cell_lanes;
     a.err = &c->d_hdr->err;
     a.act = c->receptor_act;
-    // The throughput form for large populations (plain mode only; see
-    // marl_ctx_set_cell_form).
-    a.lean = c->cell_form == MARL_CELL_FORM_THROUGHPUT ||
-             (c->cell_form == MARL_CELL_FORM_AUTO && !c->n_on_device && c->n >= kLeanCells);
     return a;
 }
 
@@ -542,14 +538,6 @@ marl_status marl_ctx_set_cell_lanes(marl_ctx* c, uint32_t lanes) {
     if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
     if (lanes < 1 || lanes > 32) return fail(MARL_ERR_INVALID_INPUT, "lanes %u outside 1..32", lanes);
     c->cell_lanes = lanes;
-    return MARL_OK;
-}
-
-marl_status marl_ctx_set_cell_form(marl_ctx* c, int32_t form) {
-    if (!c) return fail(MARL_ERR_INVALID_INPUT, "null ctx");
-    if (form < MARL_CELL_FORM_AUTO || form > MARL_CELL_FORM_THROUGHPUT)
-        return fail(MARL_ERR_INVALID_INPUT, "cell form %d", form);
-    c->cell_form = form;
     return MARL_OK;
 }
 

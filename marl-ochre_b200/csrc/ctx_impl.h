@@ -13,9 +13,6 @@
 namespace marl {
 
 constexpr uint32_t kPrefetchChanges = 256;  // change-list entries fetched with the header
-// Populations from which MARL_CELL_FORM_AUTO runs the plain cell loop in its
-// throughput form.
-constexpr uint32_t kLeanCells = 131072;
 
 }  // namespace marl
 
@@ -38,7 +35,6 @@ struct marl_ctx {
     bool c4_valid = false;     // c4 equals species 4 of field[cur]
     marl::CellTable t{};
     uint32_t cell_lanes = 32;  // cells per warp ticket of the cell loop
-    int cell_form = 0;         // MARL_CELL_FORM_* (marl_ctx_set_cell_form)
     uint32_t wait_limit = marl::kFlagSpinLimit;  // polls of a dependency flag (marl_ctx_set_wait_limit)
     int32_t hold_cell = -1;    // marl_ctx_test_hold_dependency: cell, face and slot for the next phase
     int hold_face = 0;

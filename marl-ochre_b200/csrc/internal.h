@@ -152,7 +152,6 @@ struct CellLaunch {
     uint32_t* ticket;
     uint32_t* err;
     float* act = nullptr;  // receptor activations [8][cap] of the cells updated (nullable)
-    bool lean = false;     // plain mode: the throughput form (ruleset read where used, less shared memory)
 };
 
 cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s);

@@ -188,7 +188,6 @@ def write_dump(directory: str, tick: int, dims, field: np.ndarray | None, cells:
 
 
 RULESETS_LAYERS, RULESETS_FULL, RULESETS_BOTH = 1, 2, 3
-CELL_FORM_AUTO, CELL_FORM_LATENCY, CELL_FORM_THROUGHPUT = 0, 1, 2
 
 
 def ctx_write_ruleset_dumps(ctx_handle, directory: str, tick: int, mode: int = RULESETS_BOTH) -> None:
@@ -218,7 +217,7 @@ LIB_PATH = os.path.join(HERE, "libmarl_cuda.so")
 EXPORTED = [
     "marl_sim_params_default", "marl_last_error", "marl_abi_version",
     "marl_ctx_create", "marl_ctx_destroy", "marl_ctx_set_stream", "marl_ctx_set_params", "marl_ctx_synchronize",
-    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_set_cell_lanes", "marl_ctx_set_cell_form", "marl_ctx_set_wait_limit",
+    "marl_ctx_set_tile", "marl_ctx_get_tile", "marl_ctx_set_cell_lanes", "marl_ctx_set_wait_limit",
     "marl_ctx_test_hold_dependency", "marl_ctx_set_receptor_output", "marl_ctx_download_receptor_activations",
     "marl_ctx_hgt", "marl_ctx_autotune", "marl_ctx_counters",
     "marl_upload_field", "marl_download_field", "marl_upload_light", "marl_download_light",
@@ -270,7 +269,6 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_set_tile": (c_int32, [P, c_int32, c_int32]),
         "marl_ctx_get_tile": (c_int32, [P, POINTER(c_int32), POINTER(c_int32)]),
         "marl_ctx_set_cell_lanes": (c_int32, [P, c_uint32]),
-        "marl_ctx_set_cell_form": (c_int32, [P, c_int32]),
         "marl_ctx_set_wait_limit": (c_int32, [P, c_uint32]),
         "marl_ctx_test_hold_dependency": (c_int32, [P, c_uint32, c_uint32, c_uint32]),
         "marl_ctx_set_receptor_output": (c_int32, [P, c_int32]),
@@ -442,10 +440,6 @@ class Context:
 
     def set_tile(self, tile: int, zc: int) -> None:
         _check(self.lib.marl_ctx_set_tile(self.h, tile, zc), "marl_ctx_set_tile")
-
-    def set_cell_form(self, form: int) -> None:
-        """CELL_FORM_AUTO / CELL_FORM_LATENCY / CELL_FORM_THROUGHPUT for the plain cell loop."""
-        _check(self.lib.marl_ctx_set_cell_form(self.h, form), "marl_ctx_set_cell_form")
 
     def set_receptor_output(self, enable: bool = True) -> None:
         """Phase 1 (receptor activations) as an output of every later cell phase."""

@@ -13,10 +13,7 @@ from helpers import clustered_positions, random_cells, random_field
 pytestmark = pytest.mark.gpu
 
 
-FORMS = [1, 2]  # the latency and the throughput form of the plain cell loop (marl_ctx_set_cell_form)
-
-
-def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32, form=0):
+def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32):
     rng = np.random.default_rng(seed)
     X, Y, Z = dims
     f = random_field(dims, rng)
@@ -24,7 +21,6 @@ def run_cell_phase(marl, oracle_mod, dims, cells, seed, lanes=32, form=0):
     p = marl.default_params()
     ctx = marl.Context(dims, p, cell_capacity=max(len(cells), 1))
     marl._check(marl.load().marl_ctx_set_cell_lanes(ctx.h, lanes), "marl_ctx_set_cell_lanes")
-    ctx.set_cell_form(form)
     ctx.upload_field(f)
     ctx.upload_light(light)
     ctx.upload_cells(cells)
@@ -47,25 +43,23 @@ def assert_same(gpu, cpu):
     assert gc["ruleset"].tobytes() == cc["ruleset"].tobytes()
 
 
-@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("n", [1, 7, 300])
-def test_cell_phase_sparse(marl, oracle_mod, n, form):
+def test_cell_phase_sparse(marl, oracle_mod, n):
     dims = (32, 24, 16)
     cells = random_cells(dims, n, np.random.default_rng(n))
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, n, form=form)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, n)
     assert_same(gpu, cpu)
 
 
-@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("lanes", [1, 5, 8, 16])
-def test_cell_phase_cells_per_warp(marl, oracle_mod, lanes, form):
+def test_cell_phase_cells_per_warp(marl, oracle_mod, lanes):
     """Fewer cells per warp ticket (marl_ctx_set_cell_lanes) leave the result
     unchanged: dense blobs, long dependency chains."""
     dims = (24, 20, 16)
     rng = np.random.default_rng(31)
     pos = clustered_positions(dims, 0.5, rng, 1, 3)
     cells = random_cells(dims, len(pos), rng, positions=pos)
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 78, lanes=lanes, form=form)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 78, lanes=lanes)
     assert_same(gpu, cpu)
 
 
@@ -77,20 +71,18 @@ def test_cell_lanes_rejects_out_of_range(marl):
     assert lib.marl_ctx_set_cell_lanes(ctx.h, 32) == 0
 
 
-@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("frac", [0.05, 0.3, 0.7])
-def test_cell_phase_clustered(marl, oracle_mod, frac, form):
+def test_cell_phase_clustered(marl, oracle_mod, frac):
     """Clustered blobs: many cells share empty voxels, long dependency chains."""
     dims = (24, 20, 16)
     rng = np.random.default_rng(int(frac * 100))
     pos = clustered_positions(dims, frac, rng, 1, 3)
     cells = random_cells(dims, len(pos), rng, positions=pos)
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 77, form=form)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 77)
     assert_same(gpu, cpu)
 
 
-@pytest.mark.parametrize("form", FORMS)
-def test_cell_phase_chain_order(marl, oracle_mod, form):
+def test_cell_phase_chain_order(marl, oracle_mod):
     """Cells in a line with one-voxel gaps: every cell depends on its predecessor."""
     dims = (64, 1, 1)
     xs = np.arange(0, 64, 2)
@@ -98,23 +90,21 @@ def test_cell_phase_chain_order(marl, oracle_mod, form):
     order = rng.permutation(len(xs))  # scrambled Vec order
     pos = np.stack([xs[order], np.zeros_like(xs), np.zeros_like(xs)], 1)
     cells = random_cells(dims, len(pos), rng, positions=pos)
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 5, form=form)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 5)
     assert_same(gpu, cpu)
 
 
-@pytest.mark.parametrize("form", [0, 1, 2])
-def test_cell_phase_many_cells(marl, oracle_mod, form):
+def test_cell_phase_many_cells(marl, oracle_mod):
     """Cell-kinetics microbenchmark shape at reduced size: 11.9% random occupancy."""
     dims = (64, 64, 48)
     n = int(0.119 * 64 * 64 * 48)
     cells = random_cells(dims, n, np.random.default_rng(2024))
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 2024, form=form)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 2024)
     assert_same(gpu, cpu)
 
 
-@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("seed", [31, 32, 33])
-def test_cell_phase_edge_rulesets(marl, oracle_mod, form, seed):
+def test_cell_phase_edge_rulesets(marl, oracle_mod, seed):
     """Rulesets that take every branch of the transport, reaction and effector
     order: transporters and effectors sharing a species, invalid indices
     (species out of range skip the slot), reactions whose cofactor is their
@@ -158,7 +148,7 @@ def test_cell_phase_edge_rulesets(marl, oracle_mod, form, seed):
     vm[rng.random((n, 16)) < 0.1] = 0.0
     bad = rng.random((n, 16)) < 0.05
     rx["catalyst"][bad] = rng.integers(16, 256, bad.sum())
-    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, seed, form=form)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, seed)
     assert_same(gpu, cpu)
 
 

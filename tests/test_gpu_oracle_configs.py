@@ -93,8 +93,7 @@ def test_field_microbench_full_size(marl, oracle_mod, mode):
     np.testing.assert_allclose(got_light, want_light, rtol=1e-5, atol=1e-6)
 
 
-@pytest.mark.parametrize("form", [1, 2])
-def test_cell_microbench_full_size(marl, oracle_mod, form):
+def test_cell_microbench_full_size(marl, oracle_mod):
     import workloads
 
     dims = workloads.MICRO_DIMS
@@ -103,7 +102,6 @@ def test_cell_microbench_full_size(marl, oracle_mod, form):
     cells = workloads.cell_microbench()
     p = marl.default_params()
     ctx = marl.Context(dims, p, cell_capacity=len(cells))
-    ctx.set_cell_form(form)  # latency and throughput forms of the loop
     ctx.upload_field(field)
     ctx.upload_cells(cells)
     ctx.light_update()  # one light scan on the cells' occupancy
