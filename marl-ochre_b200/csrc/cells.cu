@@ -173,7 +173,9 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S,
     pre.state = t.state[j];
     pre.age = t.age[j];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) pre.dep[f] = ((pre.nb >> f) & 1u) ? t.dep[(size_t)f * cap + j] : -1;
+    // The schedule stores -1 for faces that are not empty in-grid voxels, so
+    // the six loads need not wait for nb.
+    for (int f = 0; f < 6; ++f) pre.dep[f] = t.dep[(size_t)f * cap + j];
     const Grid g = v.g;
     pre.light = v.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
 }
