@@ -619,7 +619,7 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kTickThreads, 3) k_cell_tick(const __grid_constant__ CellLaunch a) {
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constant__ CellLaunch a) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const uint32_t total = a.n_dev ? *a.n_dev : a.n;
@@ -727,7 +727,7 @@ __global__ void k_surrogate_count(const uint8_t* __restrict__ status, const floa
 // cell j is ticket cell_base(r) + j), so every dependency of a cell, which lies
 // in the same run at a smaller index, also has a smaller ticket.
 template <int MODE>
-__global__ void __launch_bounds__(kTickThreads, 3) k_cell_tick_batch(const RunDesc* __restrict__ runs, int n_runs,
+__global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc* __restrict__ runs, int n_runs,
                                                                   BatchScalars* __restrict__ bs, CellConsts c,
                                                                   int parity) {
     extern __shared__ __align__(16) unsigned char tick_smem[];
@@ -1111,10 +1111,6 @@ static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaS
     cudaError_t e = setup_once(setup, &per_sm, [](int* v) {
         cudaError_t r = cudaFuncSetAttribute(k_cell_tick<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
         if (r != cudaSuccess) return r;
-        // Three blocks of 75.8 KB fit only with the whole carveout as shared memory.
-        r = cudaFuncSetAttribute(k_cell_tick<MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
-        if (r != cudaSuccess) return r;
         r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick<MODE>, kTickThreads, kTickSmem);
         if (*v < 1) *v = 1;
         return r;
@@ -1240,9 +1236,6 @@ static cudaError_t launch_cell_tick_batch_mode(const RunDesc* runs, int n_runs, 
     cudaError_t e = setup_once(setup, &per_sm, [](int* v) {
         cudaError_t r =
             cudaFuncSetAttribute(k_cell_tick_batch<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTickSmem);
-        if (r != cudaSuccess) return r;
-        r = cudaFuncSetAttribute(k_cell_tick_batch<MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
         if (r != cudaSuccess) return r;
         r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick_batch<MODE>, kTickThreads, kTickSmem);
         if (*v < 1) *v = 1;
