@@ -97,8 +97,8 @@ __global__ void k_cell_schedule_batch(const RunDesc* __restrict__ runs, int n_ru
 constexpr int kTickThreads = 128;
 
 // Per-thread staging, [item][thread] so that dynamic indices never cause bank
-// conflicts: the cell's ruleset and internal state are copied in with cp.async
-// (independent loads in flight together) while the neighbour gather runs.
+// conflicts: everything a cell's update reads from the cell table is copied in
+// with cp.async (independent loads in flight together, no registers held).
 struct CellScratch {
     uint4 rx[MARL_R_MAX][kTickThreads];
     float2 tp[MARL_S_TRANSPORTERS][kTickThreads];
@@ -108,6 +108,7 @@ struct CellScratch {
     float x[MARL_M_INT][kTickThreads];
     float ext[MARL_S_EXT][kTickThreads];
     float del[MARL_S_EXT][kTickThreads];
+    uint32_t hdr[10][kTickThreads];  // nb, pos, state, age, dep[0..5]
 };
 constexpr int kTickSmem = (int)sizeof(CellScratch);
 
@@ -120,9 +121,8 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ void st4(float* p, float4 v) { __stcg(reinterpret_cast<float4*>(p), v); }
@@ -133,13 +133,20 @@ __device__ __forceinline__ float rclamp(float v, float lo, float hi) {  // Rust 
     return v;
 }
 
-// Everything a cell's update needs that no other cell of this tick writes:
-// staged before the cell waits on its dependencies.
+// The staged schedule and state words of a cell (no other cell of this tick
+// writes them).
 struct CellPre {
     uint32_t nb, pos, state, age;
-    float light;
-    int32_t dep[6];
 };
+
+__device__ __forceinline__ CellPre staged_pre(const CellScratch& S) {
+    const int tid = threadIdx.x;
+    return CellPre{S.hdr[0][tid], S.hdr[1][tid], S.hdr[2][tid], S.hdr[3][tid]};
+}
+
+__device__ __forceinline__ int32_t staged_dep(const CellScratch& S, int f) {
+    return (int32_t)S.hdr[4 + f][threadIdx.x];
+}
 
 // What one lane needs to know about the run its cell belongs to.
 struct CellRunView {
@@ -152,11 +159,12 @@ struct CellRunView {
     float* act;          // receptor activations [8][cap], or null
 };
 
-__device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j, CellPre& pre) {
+// Issues (and commits as one group) the asynchronous copies of cell j's table
+// entries into the lane's staging slots; cp_async_wait_all() completes them.
+__device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j) {
     const int tid = threadIdx.x;
     const CellTable& t = *v.t;
     const size_t cap = t.cap;
-    // Ruleset and internal state: asynchronous copies into shared memory.
 #pragma unroll
     for (int r = 0; r < MARL_R_MAX; ++r) cp_async16(&S.rx[r][tid], &t.rx[r * cap + j]);
 #pragma unroll
@@ -168,25 +176,23 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S,
     cp_async16(&S.fate[tid], &t.fate[j]);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) cp_async4(&S.x[k][tid], &t.internal[k * cap + j]);
-    pre.nb = t.nb[j];
-    pre.pos = t.pos[j];
-    pre.state = t.state[j];
-    pre.age = t.age[j];
+    cp_async4(&S.hdr[0][tid], &t.nb[j]);
+    cp_async4(&S.hdr[1][tid], &t.pos[j]);
+    cp_async4(&S.hdr[2][tid], &t.state[j]);
+    cp_async4(&S.hdr[3][tid], &t.age[j]);
+    // The schedule stores -1 for faces that are not empty in-grid voxels.
 #pragma unroll
-    // The schedule stores -1 for faces that are not empty in-grid voxels, so
-    // the six loads need not wait for nb.
-    for (int f = 0; f < 6; ++f) pre.dep[f] = t.dep[(size_t)f * cap + j];
-    const Grid g = v.g;
-    pre.light = v.light[((size_t)pos_z(pre.pos) * g.Y + pos_y(pre.pos)) * g.X + pos_x(pre.pos)];
+    for (int f = 0; f < 6; ++f) cp_async4(&S.hdr[4 + f][tid], &t.dep[(size_t)f * cap + j]);
+    cp_async_commit();
 }
 
-// Gather and transport of cell j (spatial.rs:56-77, cell.rs:223-243): the
-// neighbour mean into S.ext, S.del zeroed then holding the transport deltas,
-// S.x the internal state after transport with the light in slot 15.  Shared
-// by the cell loop and the surrogate's pre-pass, so both produce the same bits
-// from the same field.
-__device__ __forceinline__ void gather_transport(const CellRunView& v, const CellConsts& c, CellScratch& S,
-                                                 const CellPre& pre, float4 (&nv)[6][3]) {
+// Gather and transport of the staged cell (spatial.rs:56-77, cell.rs:223-243):
+// the neighbour mean into S.ext, S.del zeroed then holding the transport
+// deltas, S.x the internal state after transport with the light in slot 15.
+// Returns the light at the cell's voxel.  Shared by the cell loop and the
+// surrogate's pre-pass, so both produce the same bits from the same field.
+__device__ __forceinline__ float gather_transport(const CellRunView& v, const CellConsts& c, CellScratch& S,
+                                                  const CellPre& pre, float4 (&nv)[6][3]) {
     const int tid = threadIdx.x;
     const Grid g = v.g;
     const uint32_t nb = pre.nb;
@@ -196,20 +202,27 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
     const long long off[6] = {1, -1, (long long)g.X, -(long long)g.X, (long long)g.X * g.Y,
                               -(long long)g.X * g.Y};
     const int n = __popc(nb);
-    const float light = pre.light;
+    const float light = __ldg(v.light + vox);
 
     // Gather: mean of the empty face neighbours (spatial.rs:56-77), summed in
     // face order from 0.0.  Dividing by n = 1, 2 or 4 is done as an exact
     // multiplication (a power-of-two divisor gives the identical IEEE result).
+    // All neighbour loads are issued before the first sum, so they are in
+    // flight together.
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if ((nb >> f) & 1u) {
+            const float* src = v.field + (size_t)((long long)vox + off[f]) * 12;
+            nv[f][0] = ld4(src), nv[f][1] = ld4(src + 4), nv[f][2] = ld4(src + 8);
+        }
+    }
     float acc[12];
 #pragma unroll
     for (int s = 0; s < 12; ++s) acc[s] = 0.0f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (!((nb >> f) & 1u)) continue;
-        const float* src = v.field + (size_t)((long long)vox + off[f]) * 12;
-        const float4 q0 = ld4(src), q1 = ld4(src + 4), q2 = ld4(src + 8);
-        nv[f][0] = q0, nv[f][1] = q1, nv[f][2] = q2;
+        const float4 q0 = nv[f][0], q1 = nv[f][1], q2 = nv[f][2];
         const float vals[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 #pragma unroll
         for (int s = 0; s < 12; ++s) acc[s] = acc[s] + vals[s];
@@ -231,7 +244,6 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
 #pragma unroll
     for (int s = 0; s < 12; ++s) S.del[s][tid] = 0.0f;
     const float dt = c.dt;
-    cp_async_wait_all();
 
     // Phase 2: transport (cell.rs:223-238).  Uptake depends only on the
     // gathered environment, so all eight are evaluated first; secretion
@@ -251,13 +263,16 @@ __device__ __forceinline__ void gather_transport(const CellRunView& v, const Cel
         const uint32_t e = pair & 0xFF, k = pair >> 8;
         if (e >= MARL_S_EXT || k >= MARL_M_INT) continue;
         const float2 r = S.tp[i][tid];
+        // Both operands of the transporter are read before either is written.
         const float xk = S.x[k][tid];
+        const float de = S.del[e][tid];
         const float uptake = uptakes[i];
         const float secretion = div_rn(r.y * xk, 1.0f + xk);
         S.x[k][tid] = rclamp(xk + (uptake - secretion) * dt, 0.0f, c.c_max);
-        S.del[e][tid] = S.del[e][tid] + (secretion - uptake) * dt;
+        S.del[e][tid] = de + (secretion - uptake) * dt;
     }
     S.x[MARL_M_INT - 1][tid] = light;  // cell.rs:243
+    return light;
 }
 
 // Phase 1 of CellState::tick (cell.rs:206-220): receptor i's Hill activation
@@ -290,29 +305,41 @@ __device__ __forceinline__ int reactions(const CellConsts& c, CellScratch& S) {
     const float dt = c.dt;
     const float feps = 1.1920928955078125e-07f;
     int active = 0;
+    // The next reaction's record is loaded while the current one runs.
+    uint4 qn = S.rx[0][tid];
 #pragma unroll 4
     for (int r = 0; r < MARL_R_MAX; ++r) {
-        const uint4 q = S.rx[r][tid];
+        const uint4 q = qn;
+        if (r + 1 < MARL_R_MAX) qn = S.rx[r + 1][tid];
         const uint32_t si = q.x & 0xFF, pi = (q.x >> 8) & 0xFF, ci = (q.x >> 16) & 0xFF, fi = q.x >> 24;
         const float km = __uint_as_float(q.y), vmax = __uint_as_float(q.z), kcat = __uint_as_float(q.w);
         if (fabsf(vmax) > c.thr && si != pi) ++active;
         if (fabsf(vmax) < c.thr) continue;
         if (si == pi) continue;
         if (si >= MARL_M_INT || pi >= MARL_M_INT || ci >= MARL_M_INT) continue;
+        const bool has_cof = fi != MARL_NO_COFACTOR && fi < MARL_M_INT;
+        // The reaction's operands are read together before any is written;
+        // its own writes are forwarded in registers (the cofactor's new value
+        // is what a later read of the same species would see).
         const float s = S.x[si][tid];
         const float cc = S.x[ci][tid];
+        const float p = S.x[pi][tid];
+        const float cof = has_cof ? S.x[fi][tid] : 0.0f;
         const float substrate_term = div_rn(s, km + s + feps);
         const float catalyst_term = c.epsilon + div_rn(cc, kcat + cc + feps);
         float rate = vmax * substrate_term * catalyst_term;
-        if (fi != MARL_NO_COFACTOR && fi < MARL_M_INT) {
-            const float cof = S.x[fi][tid];
+        float s_now = s, p_now = p;
+        if (has_cof) {
             rate *= div_rn(cof, 1.0f + cof);
-            const float consumed = fminf(0.5f * rate * dt, S.x[fi][tid]);
-            S.x[fi][tid] = S.x[fi][tid] - consumed;
+            const float consumed = fminf(0.5f * rate * dt, cof);
+            const float cof_left = cof - consumed;
+            S.x[fi][tid] = cof_left;
+            if (fi == si) s_now = cof_left;
+            if (fi == pi) p_now = cof_left;
         }
-        const float flux = fminf(rate * dt, S.x[si][tid]);
-        S.x[si][tid] = S.x[si][tid] - flux;
-        S.x[pi][tid] = fminf(S.x[pi][tid] + flux, c.c_max);
+        const float flux = fminf(rate * dt, s_now);
+        S.x[si][tid] = s_now - flux;
+        S.x[pi][tid] = fminf(p_now + flux, c.c_max);
     }
     return active;
 }
@@ -381,10 +408,11 @@ __device__ __forceinline__ void maintenance_effectors(const CellConsts& c, CellS
             if (k >= MARL_M_INT || e >= MARL_S_EXT) continue;
             const float2 pr = S.ef[i][tid];
             const float xk = S.x[k][tid];
+            const float de = S.del[e][tid];
             if (xk > pr.x) {
                 const float amount = div_rn(pr.y * xk, 1.0f + xk) * dt;
                 S.x[k][tid] = fmaxf(xk - amount, 0.0f);
-                S.del[e][tid] = S.del[e][tid] + amount;
+                S.del[e][tid] = de + amount;
             }
         }
     }
@@ -395,10 +423,10 @@ __device__ __forceinline__ void maintenance_effectors(const CellConsts& c, CellS
 // row), kModeGated / kModeTrusted (reaction phase from the surrogate where
 // the pre-pass speculation holds; see SurrView).
 template <int MODE>
-__device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
-                            const CellPre& pre) {
+__device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j) {
     const int tid = threadIdx.x;
     const CellTable& t = *v.t;
+    const CellPre pre = staged_pre(S);
     const Grid g = v.g;
     const uint32_t nb = pre.nb;
     const uint32_t P = pre.pos;
@@ -415,7 +443,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     // The gathered neighbour values are also the scatter's starting values:
     // no other cell touches N(j) while this cell holds it.
     float4 nv[6][3];
-    gather_transport(v, c, S, pre, nv);
+    const float light = gather_transport(v, c, S, pre, nv);
     if (v.act) receptor_activations(c, t, j, S, v.act);
 
     int active;
@@ -426,7 +454,7 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
         const SurrView& sv = *v.sv;
         const bool cap_row = j < sv.raw_rows;
         float* row = sv.raw + (size_t)j * MARL_SURR_RAW_STRIDE;
-        if (cap_row) surrogate_features(S, pre.light, [&](int f, float val) { row[f] = val; });
+        if (cap_row) surrogate_features(S, light, [&](int f, float val) { row[f] = val; });
         active = reactions(c, S);
         if (cap_row) {
 #pragma unroll
@@ -557,11 +585,17 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
     for (int k = 0; k < MARL_M_INT; ++k) t.internal[(size_t)k * t.cap + j] = S.x[k][tid];
 }
 
-// The ticket loop shared by the single-run and the batched kernel.  `resolve`
+// The ticket loops shared by the single-run and the batched kernel.  `resolve`
 // maps a ticket (global cell index) to the lane's run view and local index.
+//
+// Warp tickets: each warp takes `lanes` consecutive cells, stages them, and
+// updates each as soon as its dependencies are done; it takes the next ticket
+// when all of them are finished.  Used when every cell gets a lane at once
+// (the grid's lanes cover the cells), where it is the shortest path.
 template <int MODE, class Resolve>
-__device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts& c, uint32_t total, uint32_t* ticket,
-                                               uint32_t* err, uint32_t lanes, Resolve resolve) {
+__device__ __forceinline__ void cell_tick_loop_tickets(CellScratch& S, const CellConsts& c, uint32_t total,
+                                                       uint32_t* ticket, uint32_t* err, uint32_t lanes,
+                                                       Resolve resolve) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -573,30 +607,31 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
         bool pending = (uint32_t)lane < lanes && gi < total;
         CellRunView v{};
         uint32_t j = 0;
-        CellPre pre;
         if (pending) {
             resolve(gi, v, j);
-            stage_cell(v, S, j, pre);
+            stage_cell(v, S, j);
         }
+        cp_async_wait_all();
         // Dependencies not yet seen finished (bit f: face f).  A poll loads
         // them with relaxed loads, all in flight together; once every one has
         // been seen, one acquire fence orders the update after the writers.
         uint32_t remaining = 0;
 #pragma unroll
-        for (int f = 0; f < 6; ++f) remaining |= (pending && pre.dep[f] >= 0 ? 1u : 0u) << f;
+        for (int f = 0; f < 6; ++f) remaining |= (pending && staged_dep(S, f) >= 0 ? 1u : 0u) << f;
         uint32_t spins = 0;
         while (__any_sync(FULL, pending)) {
             if (pending) {
                 const CellTable& t = *v.t;
                 uint32_t seen[6];
 #pragma unroll
-                for (int f = 0; f < 6; ++f) seen[f] = ((remaining >> f) & 1u) ? ld_relaxed_u32(&t.done[pre.dep[f]]) : 0u;
+                for (int f = 0; f < 6; ++f)
+                    seen[f] = ((remaining >> f) & 1u) ? ld_relaxed_u32(&t.done[staged_dep(S, f)]) : 0u;
 #pragma unroll
                 for (int f = 0; f < 6; ++f)
                     if (((remaining >> f) & 1u) && seen[f] == v.epoch) remaining &= ~(1u << f);
                 if (remaining == 0) {
                     fence_acquire_gpu();
-                    update_cell<MODE>(v, c, S, j, pre);  // publishes done[j] itself
+                    update_cell<MODE>(v, c, S, j);  // publishes done[j] itself
                     pending = false;
                 }
             }
@@ -605,7 +640,6 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
                     if (pending) {
                         const CellTable& t = *v.t;
                         atomicOr(err, kErrTimeoutDeps);
-                        cp_async_wait_all();  // drain this lane's staging copies
                         t.events[j] = MARL_EVENT_NONE;
                         st_release_u32(&t.done[j], v.epoch);
                         pending = false;
@@ -616,6 +650,98 @@ __device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts&
             }
         }
     }
+}
+
+// Lane refill: each warp keeps up to `lanes` cells in flight, one per lane,
+// and works in rounds: poll the dependencies of its staged cells, update the ready ones
+// together, then hand every lane that is free the next index from the ticket
+// counter (in lane order, so indices still go out in ascending order) and
+// stage its cell.  A cell whose dependency is still running holds only its
+// own lane; the other lanes move on to new cells.  Staging writes only shared
+// memory (cp.async), and its copies are awaited at the start of the next
+// round, so an update never waits on another lane's loads.  The ticket request
+// is sent before the updates and its reply is read after them.
+template <int MODE, class Resolve>
+__device__ __forceinline__ void cell_tick_loop_refill(CellScratch& S, const CellConsts& c, uint32_t total,
+                                                      uint32_t* ticket, uint32_t* err, uint32_t lanes,
+                                                      Resolve resolve) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const bool usable = (uint32_t)lane < lanes;
+    constexpr uint32_t kUnscanned = 1u << 6;  // dependencies of a fresh cell not yet read
+    bool pending = false, more = true;
+    uint32_t gi = 0, remaining = 0, spins = 0;
+    for (;;) {
+        cp_async_wait_all();  // the previous round's staging
+        bool ready = false;
+        CellRunView v{};
+        uint32_t j = 0;
+        if (pending) {
+            resolve(gi, v, j);
+            if (remaining & kUnscanned) {
+                remaining = 0;
+#pragma unroll
+                for (int f = 0; f < 6; ++f) remaining |= (staged_dep(S, f) >= 0 ? 1u : 0u) << f;
+            }
+            // The remaining flags, loaded relaxed and all in flight together;
+            // once every one has been seen, one acquire fence orders the
+            // update after the writers.
+            const CellTable& t = *v.t;
+            uint32_t seen[6];
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                seen[f] = ((remaining >> f) & 1u) ? ld_relaxed_u32(&t.done[staged_dep(S, f)]) : 0u;
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if (((remaining >> f) & 1u) && seen[f] == v.epoch) remaining &= ~(1u << f);
+            ready = remaining == 0;
+        }
+        const unsigned freed = __ballot_sync(FULL, usable && (!pending || ready));
+        uint32_t base = 0;
+        if (more && freed && lane == 0) base = atomicAdd(ticket, (uint32_t)__popc(freed));
+        if (ready) {
+            fence_acquire_gpu();
+            update_cell<MODE>(v, c, S, j);  // publishes done[j] itself
+            pending = false;
+        } else if (pending && ++spins > c.wait_limit) {
+            const CellTable& t = *v.t;
+            atomicOr(err, kErrTimeoutDeps);
+            t.events[j] = MARL_EVENT_NONE;
+            st_release_u32(&t.done[j], v.epoch);
+            pending = false;
+        }
+        if (more && freed) {
+            base = __shfl_sync(FULL, base, 0);
+            if (base >= total) {
+                more = false;
+            } else if ((freed >> lane) & 1u) {
+                const uint32_t next = base + (uint32_t)__popc(freed & ((1u << lane) - 1u));
+                if (next < total) {
+                    gi = next;
+                    resolve(gi, v, j);
+                    stage_cell(v, S, j);
+                    pending = true;
+                    spins = 0;
+                    remaining = kUnscanned;
+                }
+            }
+        }
+        if (!__any_sync(FULL, pending)) break;
+        // Back off only when no lane of the warp made progress this round.
+        if (!__any_sync(FULL, ready)) __nanosleep(64);
+    }
+}
+
+// Warp tickets when the grid's lanes cover every cell, lane refill otherwise
+// (the choice is uniform over the grid: it depends only on the cell count).
+template <int MODE, class Resolve>
+__device__ __forceinline__ void cell_tick_loop(CellScratch& S, const CellConsts& c, uint32_t total, uint32_t* ticket,
+                                               uint32_t* err, uint32_t lanes, Resolve resolve) {
+    const uint64_t grid_lanes = (uint64_t)gridDim.x * (kTickThreads / 32) * lanes;
+    if (total <= grid_lanes)
+        cell_tick_loop_tickets<MODE>(S, c, total, ticket, err, lanes, resolve);
+    else
+        cell_tick_loop_refill<MODE>(S, c, total, ticket, err, lanes, resolve);
 }
 
 template <int MODE>
@@ -635,16 +761,17 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constan
 __device__ __forceinline__ void prepass_cell(const CellRunView& v, const CellConsts& c, CellScratch& S, uint32_t j,
                                              uint32_t row, size_t ld, const float* __restrict__ norm,
                                              float* __restrict__ xt, __nv_bfloat16* __restrict__ X) {
-    CellPre pre;
-    stage_cell(v, S, j, pre);
+    stage_cell(v, S, j);
+    cp_async_wait_all();
+    const CellPre pre = staged_pre(S);
     float4 nv[6][3];
-    gather_transport(v, c, S, pre, nv);
+    const float light = gather_transport(v, c, S, pre, nv);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) xt[k * ld + row] = S.x[k][threadIdx.x];
     float f[mlp::kInPad];
 #pragma unroll
     for (int i = mlp::kIn; i < mlp::kInPad; ++i) f[i] = 0.0f;
-    surrogate_features(S, pre.light, [&](int i, float val) {
+    surrogate_features(S, light, [&](int i, float val) {
         f[i] = (mlp::feature_transform(i, val) - norm[i]) / norm[mlp::kIn + i];
     });
     uint4* dst = reinterpret_cast<uint4*>(X + (size_t)row * mlp::kInPad);

@@ -63,6 +63,20 @@ def test_cell_phase_cells_per_warp(marl, oracle_mod, lanes):
     assert_same(gpu, cpu)
 
 
+@pytest.mark.parametrize("lanes,frac", [(1, 0.3), (1, 0.7), (4, 0.5), (32, 0.5)])
+def test_cell_phase_lane_refill(marl, oracle_mod, lanes, frac):
+    """More cells than the grid has lanes: warps hand finished lanes the next
+    cells while other lanes wait on dependencies (lane refill).  With one or
+    four cells per warp this happens at a few thousand cells; with 32 the
+    grid covers every cell of this population at once (warp tickets)."""
+    dims = (40, 32, 24)
+    rng = np.random.default_rng(int(frac * 10) + lanes)
+    pos = clustered_positions(dims, frac, rng, 1, 3)
+    cells = random_cells(dims, len(pos), rng, positions=pos)
+    gpu, cpu = run_cell_phase(marl, oracle_mod, dims, cells, 90 + lanes, lanes=lanes)
+    assert_same(gpu, cpu)
+
+
 def test_cell_lanes_rejects_out_of_range(marl):
     ctx = marl.Context((8, 8, 8), marl.default_params(), cell_capacity=8)
     lib = marl.load()

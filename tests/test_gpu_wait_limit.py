@@ -92,3 +92,46 @@ def test_hold_through_occupied_face_is_reported(marl):
         ctx.cell_phase()
     assert e.value.status_name == "INVALID_INPUT"
     ctx.close()
+
+
+def lattice_cells(dims, spacing):
+    """Cells on a lattice: no two share a neighbour voxel, all faces empty."""
+    X, Y, Z = dims
+    g = np.stack(np.meshgrid(np.arange(1, X - 1, spacing), np.arange(1, Y - 1, spacing),
+                             np.arange(1, Z - 1, spacing), indexing="ij"), -1).reshape(-1, 3)
+    cells = random_cells(dims, len(g), np.random.default_rng(8))
+    cells["pos"] = g.astype(np.uint16)
+    return cells
+
+
+def test_dependency_wait_times_out_under_lane_refill(marl, oracle_mod):
+    """The same bounded wait with more cells than lanes (one cell per warp
+    ticket), where a waiting lane stays put while the warp's other lanes take
+    new cells: the held cell gives up, every other cell is updated."""
+    dims = (62, 62, 14)
+    rng = np.random.default_rng(12)
+    f = random_field(dims, rng)
+    X, Y, Z = dims
+    light = rng.random((Z, Y, X), dtype=np.float32)
+    cells = lattice_cells(dims, 3)
+    n = len(cells)
+    assert n > 1184  # more than the lanes of a full grid at one cell per warp
+    p = marl.default_params()
+    ctx = marl.Context(dims, p, cell_capacity=n + 2)
+    marl._check(marl.load().marl_ctx_set_cell_lanes(ctx.h, 1), "marl_ctx_set_cell_lanes")
+    ctx.upload_field(f)
+    ctx.upload_light(light)
+    ctx.upload_cells(cells)
+    ctx.set_wait_limit(2000)
+    held = n // 3
+    ctx.test_hold_dependency(cell=held, face=0, slot=n + 1)
+    with pytest.raises(marl.MarlError) as e:
+        ctx.cell_phase()
+    assert e.value.status_name == "TIMEOUT"
+    got = ctx.download_cells()
+    others = np.ones(n, bool)
+    others[held] = False
+    _, cc, _ = oracle_mod.cell_phase(f, light, cells[others], dims, p)
+    np.testing.assert_array_equal(got["internal"][others], cc["internal"])
+    np.testing.assert_array_equal(got["internal"][held], cells["internal"][held])
+    ctx.close()
