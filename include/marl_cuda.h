@@ -238,10 +238,13 @@ marl_status marl_ctx_synchronize(marl_ctx* ctx);
  * Every choice gives bit-identical results; only speed differs. */
 marl_status marl_ctx_set_tile(marl_ctx* ctx, int32_t tile, int32_t zc);
 marl_status marl_ctx_get_tile(marl_ctx* ctx, int32_t* tile, int32_t* zc);
-/* Cells per warp of the cell loop (1..32, default 32): a warp takes that many
- * consecutive cells per ticket and leaves its other lanes idle.  Fewer cells
- * per warp serialise less work inside a warp along the dependency chains, at
- * the cost of more warps.  Results do not depend on it. */
+/* Cells per warp of the cell loop (1..32, default 32): a warp holds at most
+ * that many cells at once and leaves its other lanes idle.  While the grid's
+ * lanes cover every cell, a warp takes that many consecutive cells per
+ * ticket; with more cells than lanes, a lane whose cell is finished takes the
+ * next one (lane refill).  Fewer cells per warp serialise less work inside a
+ * warp along the dependency chains, at the cost of more warps.  Results do
+ * not depend on it. */
 marl_status marl_ctx_set_cell_lanes(marl_ctx* ctx, uint32_t lanes);
 /* Bound of the cell loop's dependency waits (no reference counterpart; the
  * reference loop is sequential and never waits).  A cell that has polled an
