@@ -186,4 +186,16 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
 // stores before it, it orders every later access after those stores' writers.
 __device__ __forceinline__ void fence_acquire_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization may start while the previous kernel of its stream is still
+// running, once every block of that kernel has called
+// griddep_launch_dependents (or exited).  It must not touch global memory
+// that the previous kernel reads or writes before griddep_wait() returns,
+// which is when the previous kernel has completed and its writes are
+// visible.  Without such a predecessor both are no-ops.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace marl

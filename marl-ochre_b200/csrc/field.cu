@@ -14,6 +14,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "common.cuh"
 #include "internal.h"
 #include "kernel_setup.h"
@@ -297,11 +299,16 @@ __device__ __forceinline__ void diffuse_tile(const CUtensorMap* tm_src, const CU
 
     int issued = 0, waited = 0;
     bool aborted = false;
+    // The next substep's blocks may be scheduled as soon as all of this
+    // launch's blocks are running; nothing of the previous launch's output is
+    // read or overwritten before griddep_wait.
+    griddep_launch_dependents();
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
         s_abort[0] = s_abort[1] = 0;
     }
+    griddep_wait();
     __syncthreads();
     if (tid == 0) {
         const int pre = min(STAGES, nplanes);
@@ -462,6 +469,7 @@ __global__ void __launch_bounds__(kDiffTX* TY, (diff_min_blocks<TY, DIRECT>()))
     k_diffuse_batch(const RunDesc* __restrict__ runs, const CUtensorMap* __restrict__ maps,
                     const int4* __restrict__ items, int zc, FieldConsts k, int parity, int apply_sources, int emit_c4,
                     uint32_t* __restrict__ err) {
+    griddep_wait();
     const int4 it = items[blockIdx.x];
     const RunDesc& r = runs[it.x];
     const CUtensorMap* m = maps + (size_t)it.x * kMapsPerRun;
@@ -552,6 +560,7 @@ __device__ __forceinline__ void light_columns(const float* __restrict__ c4, cons
 __global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, const float* __restrict__ field,
                                                const uint8_t* __restrict__ mask, float* __restrict__ light, Grid g,
                                                FieldConsts k) {
+    griddep_wait();  // the last substep's output
     light_columns(c4, field, mask, light, g, k, blockIdx.x * kLightCols, blockIdx.y);
 }
 
@@ -560,6 +569,7 @@ __global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, con
 // last substep, otherwise from field[parity].
 __global__ void __launch_bounds__(256) k_light_batch(const RunDesc* __restrict__ runs, const int4* __restrict__ items,
                                                      FieldConsts k, int parity, int use_c4) {
+    griddep_wait();  // the last substep's output
     const int4 it = items[blockIdx.x];
     const RunDesc& r = runs[it.x];
     light_columns(use_c4 ? r.c4 : nullptr, r.field[parity], r.mask, r.light, r.g, k, it.y * kLightCols, it.z);
@@ -648,6 +658,24 @@ void diffusion_tile_shape(int tile, int* tx, int* ty) {
     *ty = kTileTY[tile];
 }
 
+// Launch with programmatic stream serialization (the kernel calls
+// griddep_wait before it touches the previous launch's data).
+template <class... KArgs, class... Args>
+static cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                   Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <int TY, int STAGES, bool DIRECT = false>
 static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
                                     int apply_sources, float* c4_out, uint32_t* err, cudaStream_t s) {
@@ -656,10 +684,9 @@ static cudaError_t launch_diffuse_t(const DiffusionPlan& plan, int which_src, co
     cudaError_t e = set_smem_once(setup, k_diffuse<TY, STAGES, DIRECT>, T::SMEM_BYTES);
     if (e != cudaSuccess) return e;
     dim3 grid((g.X + kDiffTX - 1) / kDiffTX, (g.Y + TY - 1) / TY, (g.Z + plan.zc - 1) / plan.zc);
-    k_diffuse<TY, STAGES, DIRECT><<<grid, kDiffTX * TY, T::SMEM_BYTES, s>>>(
-        plan.tm_load[which_src], plan.tm_store[which_src ^ 1], plan.tm_mask, g, plan.zc, k, apply_sources, c4_out, err,
-        plan.buf[which_src ^ 1]);
-    return cudaGetLastError();
+    return launch_dependent(k_diffuse<TY, STAGES, DIRECT>, grid, dim3(kDiffTX * TY), T::SMEM_BYTES, s,
+                            plan.tm_load[which_src], plan.tm_store[which_src ^ 1], plan.tm_mask, g, plan.zc, k,
+                            apply_sources, c4_out, err, plan.buf[which_src ^ 1]);
 }
 
 cudaError_t launch_diffuse(const DiffusionPlan& plan, int which_src, const Grid& g, const FieldConsts& k,
@@ -689,9 +716,8 @@ static cudaError_t launch_diffuse_batch_t(const RunDesc* runs, const CUtensorMap
     static std::atomic<int> setup[kSetupDevices];
     cudaError_t e = set_smem_once(setup, k_diffuse_batch<TY, STAGES, DIRECT>, T::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    k_diffuse_batch<TY, STAGES, DIRECT><<<n_items, kDiffTX * TY, T::SMEM_BYTES, s>>>(runs, maps, items, zc, k, parity,
-                                                                                   apply_sources, emit_c4, err);
-    return cudaGetLastError();
+    return launch_dependent(k_diffuse_batch<TY, STAGES, DIRECT>, dim3(n_items), dim3(kDiffTX * TY), T::SMEM_BYTES, s,
+                            runs, maps, items, zc, k, parity, apply_sources, emit_c4, err);
 }
 
 cudaError_t launch_diffuse_batch(int tile, const RunDesc* runs, const CUtensorMap* maps, const int4* items,
@@ -716,8 +742,7 @@ cudaError_t launch_diffuse_batch(int tile, const RunDesc* runs, const CUtensorMa
 cudaError_t launch_light_batch(const RunDesc* runs, const int4* items, int n_items, const FieldConsts& k, int parity,
                                int use_c4, cudaStream_t s) {
     if (n_items == 0) return cudaSuccess;
-    k_light_batch<<<n_items, 256, 0, s>>>(runs, items, k, parity, use_c4);
-    return cudaGetLastError();
+    return launch_dependent(k_light_batch, dim3(n_items), dim3(256), 0, s, runs, items, k, parity, use_c4);
 }
 
 cudaError_t launch_sources(float* f, const Grid& g, const FieldConsts& k, cudaStream_t s) {
@@ -729,8 +754,7 @@ cudaError_t launch_sources(float* f, const Grid& g, const FieldConsts& k, cudaSt
 cudaError_t launch_light(const float* c4, const float* f, const uint8_t* mask, float* light, const Grid& g,
                          const FieldConsts& k, cudaStream_t s) {
     dim3 grid((g.X + kLightCols - 1) / kLightCols, g.Y);
-    k_light<<<grid, 256, 0, s>>>(c4, f, mask, light, g, k);
-    return cudaGetLastError();
+    return launch_dependent(k_light, grid, dim3(256), 0, s, c4, f, mask, light, g, k);
 }
 
 cudaError_t launch_mass(const float* f, const Grid& g, double* partial, double* out, cudaStream_t s) {
