@@ -14,8 +14,6 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
-#include <utility>
-
 #include "common.cuh"
 #include "internal.h"
 #include "kernel_setup.h"
@@ -560,6 +558,7 @@ __device__ __forceinline__ void light_columns(const float* __restrict__ c4, cons
 __global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, const float* __restrict__ field,
                                                const uint8_t* __restrict__ mask, float* __restrict__ light, Grid g,
                                                FieldConsts k) {
+    griddep_launch_dependents();
     griddep_wait();  // the last substep's output
     light_columns(c4, field, mask, light, g, k, blockIdx.x * kLightCols, blockIdx.y);
 }
@@ -569,6 +568,7 @@ __global__ void __launch_bounds__(256) k_light(const float* __restrict__ c4, con
 // last substep, otherwise from field[parity].
 __global__ void __launch_bounds__(256) k_light_batch(const RunDesc* __restrict__ runs, const int4* __restrict__ items,
                                                      FieldConsts k, int parity, int use_c4) {
+    griddep_launch_dependents();
     griddep_wait();  // the last substep's output
     const int4 it = items[blockIdx.x];
     const RunDesc& r = runs[it.x];
@@ -656,24 +656,6 @@ int diffusion_tile_count() { return 12; }
 void diffusion_tile_shape(int tile, int* tx, int* ty) {
     *tx = kDiffTX;
     *ty = kTileTY[tile];
-}
-
-// Launch with programmatic stream serialization (the kernel calls
-// griddep_wait before it touches the previous launch's data).
-template <class... KArgs, class... Args>
-static cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                                   Args&&... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 template <int TY, int STAGES, bool DIRECT = false>

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <utility>
 
 namespace marl {
 
@@ -46,6 +47,26 @@ cudaError_t set_smem_once(std::atomic<int>* slots, K kernel, int bytes) {
         *v = 0;
         return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     });
+}
+
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while the previous kernel of the stream drains, so it must call
+// griddep_wait (common.cuh) before it touches global memory that an earlier
+// launch writes or reads.
+template <class... KArgs, class... Args>
+cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace marl
