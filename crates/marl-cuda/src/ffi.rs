@@ -375,6 +375,7 @@ unsafe extern "C" {
     pub fn marl_fate_stream_probe(seed: u64, tick: u64, parent: u32, count: u32, stddev: f32, u64_out: *mut u64,
                                   normal_out: *mut f32) -> Status;
     pub fn marl_fate_stream_ln(x: *const f64, n: u32, out: *mut f64) -> Status;
+    pub fn marl_selftest_small_division(mismatches: *mut u64) -> Status;
 
     // statistics and snapshots
     pub fn marl_ctx_stats(ctx: *mut Ctx, out: *mut Stats, cells_per_z: *mut u32, centre_column: *mut f32)

@@ -419,6 +419,12 @@ marl_status marl_ctx_run_ticks(marl_ctx* ctx, uint32_t ticks);
 marl_status marl_fate_stream_probe(uint64_t seed, uint64_t tick, uint32_t parent, uint32_t count, float stddev,
                                    uint64_t* u64_out, float* normal_out);
 marl_status marl_fate_stream_ln(const double* x, uint32_t n, double* out);
+/* Self-test of the cell loop's division by an empty-face count of 3, 5 or 6
+ * (a reciprocal and one exact-remainder correction instead of an IEEE
+ * division): compares it bit for bit with the IEEE division for every finite
+ * float and each of the three divisors, and stores the number of differences
+ * (0 expected) in *mismatches.  Runs on the current device (about a second). */
+marl_status marl_selftest_small_division(uint64_t* mismatches);
 
 /* ---- statistics ----------------------------------------------------------
  * print_stats / print_z_profile (crates/marl-sim/src/stats.rs:9-103) reduced

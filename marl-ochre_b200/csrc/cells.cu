@@ -232,9 +232,7 @@ __device__ __forceinline__ float gather_transport(const CellRunView& v, const Ce
 #pragma unroll
         for (int s = 0; s < 12; ++s) acc[s] = acc[s] * inv;
     } else if (n > 1) {
-        const float nf = (float)n;
-#pragma unroll
-        for (int s = 0; s < 12; ++s) acc[s] = div_rn(acc[s], nf);
+        div12_small_n(acc, n);  // n = 3, 5 or 6
     }
 #pragma unroll
     for (int s = 0; s < 12; ++s) S.ext[s][tid] = acc[s];
@@ -555,9 +553,9 @@ __device__ void update_cell(const CellRunView& v, const CellConsts& c, CellScrat
 #pragma unroll
             for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid] * inv;
         } else {
-            const float nf = (float)n;
 #pragma unroll
-            for (int s = 0; s < 12; ++s) split[s] = div_rn(S.del[s][tid], nf);
+            for (int s = 0; s < 12; ++s) split[s] = S.del[s][tid];
+            div12_small_n(split, n);  // n = 3, 5 or 6
         }
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
@@ -1420,4 +1418,52 @@ cudaError_t launch_births_batch(const RunDesc* runs, const marl_cell* recs, cons
     return cudaGetLastError();
 }
 
+// Every finite float x, for n = 3, 5 and 6: the value the gather and scatter
+// use for x / n (div_small_n where div12_small_n takes it, the IEEE operator
+// otherwise) against the IEEE operator, bit for bit.
+__global__ void k_selftest_small_division(unsigned long long* __restrict__ mismatches) {
+    unsigned long long bad = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (1ull << 32); i += stride) {
+        const float x = __uint_as_float((uint32_t)i);
+        const float a = fabsf(x);
+        if (!(a <= 3.40282346638528859812e38f)) continue;  // finite only
+        const bool fast = x == 0.0f || a >= 0x1p-125f;
+#pragma unroll
+        for (int n = 3; n <= 6; ++n) {
+            if (n == 4) continue;
+            const float nf = (float)n;
+            const float got = fast ? div_small_n(x, small_divisor_inverse(n), nf) : div_rn(x, nf);
+            bad += __float_as_uint(got) != __float_as_uint(__fdiv_rn(x, nf));
+        }
+    }
+    atomicAdd(mismatches, bad);
+}
+
 }  // namespace marl
+
+#include "ctx_impl.h"
+
+using marl::check_device;
+using marl::cuda_fail;
+using marl::fail;
+
+extern "C" marl_status marl_selftest_small_division(uint64_t* mismatches) {
+    if (!mismatches) return fail(MARL_ERR_INVALID_INPUT, "null argument");
+    int dev, sms;
+    marl_status st = check_device(&dev, &sms);
+    if (st) return st;
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        marl::k_selftest_small_division<<<sms * 16, 256>>>(d);
+        e = cudaGetLastError();
+    }
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "marl_selftest_small_division");
+    *mismatches = h;
+    return MARL_OK;
+}

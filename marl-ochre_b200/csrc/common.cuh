@@ -107,6 +107,44 @@ __device__ __forceinline__ float div_rn(float a, float b) {
     return zero ? zq : q;
 }
 
+// IEEE round-to-nearest division of the 12 values v[] by the same n = 3, 5
+// or 6 (the empty-face count of a cell's gather and scatter).  With
+// c = RN(1/n), q0 = RN(x c) is within one ulp of x/n, the remainder
+// x - n q0 is exact in one FMA, and RN(q0 + r c) is the correctly rounded
+// quotient (Markstein's theorem: P. Markstein, IBM J. Res. Dev. 34(1), 1990).
+// Checked bitwise against the IEEE division over every finite float for each
+// n (marl_selftest_small_division): it differs only for -0 (kept from q0,
+// which has the right sign) and, for n = 6, below 2^-125.  So values that are
+// zero use q0, and if any value is non-zero with a magnitude below 2^-125, or
+// not finite, the 12 are divided by the IEEE operator instead.  Three
+// branch-free FMAs per value instead of a division each, which the compiler
+// would issue one after another.
+__device__ __forceinline__ float small_divisor_inverse(int n) {
+    return n == 3 ? 0x1.555556p-2f : (n == 5 ? 0x1.99999ap-3f : 0x1.555556p-3f);
+}
+__device__ __forceinline__ float div_small_n(float x, float c, float nf) {
+    const float q0 = __fmul_rn(x, c);
+    const float r = __fmaf_rn(-q0, nf, x);
+    const float q1 = __fmaf_rn(r, c, q0);
+    return x == 0.0f ? q0 : q1;
+}
+__device__ __forceinline__ void div12_small_n(float (&v)[12], int n) {
+    const float nf = (float)n, c = small_divisor_inverse(n);
+    bool exact = true;
+#pragma unroll
+    for (int s = 0; s < 12; ++s) {
+        const float a = fabsf(v[s]);
+        exact = exact && (v[s] == 0.0f || (a >= 0x1p-125f && a <= 3.40282346638528859812e38f));
+    }
+    if (exact) {
+#pragma unroll
+        for (int s = 0; s < 12; ++s) v[s] = div_small_n(v[s], c, nf);
+    } else {
+#pragma unroll
+        for (int s = 0; s < 12; ++s) v[s] = div_rn(v[s], nf);
+    }
+}
+
 // ---------------------------------------------------------------- PTX ----
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

@@ -243,6 +243,7 @@ EXPORTED = [
     "marl_write_ruleset_dumps",
     "marl_ctx_fate_init", "marl_ctx_fate", "marl_ctx_fate_stats", "marl_ctx_set_events", "marl_ctx_run_ticks",
     "marl_fate_stream_probe", "marl_fate_stream_ln", "marl_engine_set_device_fate", "marl_batch_set_device_fate",
+    "marl_selftest_small_division",
 ]
 
 _lib = None
@@ -355,6 +356,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "marl_ctx_run_ticks": (c_int32, [P, c_uint32]),
         "marl_fate_stream_probe": (c_int32, [c_uint64, c_uint64, c_uint32, c_uint32, c_float, P, P]),
         "marl_fate_stream_ln": (c_int32, [P, c_uint32, P]),
+        "marl_selftest_small_division": (c_int32, [P]),
         "marl_engine_set_device_fate": (c_int32, [P, c_int32]),
         "marl_batch_set_device_fate": (c_int32, [P, c_int32]),
     }
@@ -640,6 +642,15 @@ def fate_stream_ln(x: np.ndarray) -> np.ndarray:
     out = np.zeros(max(xs.size, 1), np.float64)
     _check(lib.marl_fate_stream_ln(_ptr(xs), xs.size, _ptr(out)), "marl_fate_stream_ln")
     return out[:xs.size]
+
+
+def selftest_small_division() -> int:
+    """marl_selftest_small_division: differences between the cell loop's
+    division by 3, 5 or 6 and the IEEE division over every finite float."""
+    lib = load()
+    out = np.zeros(1, np.uint64)
+    _check(lib.marl_selftest_small_division(_ptr(out)), "marl_selftest_small_division")
+    return int(out[0])
 
 
 def diffuse_device(field_ptr: int, scratch_ptr: int, occ_ptr: int, dims, params: SimParams, substeps: int,
