@@ -134,3 +134,44 @@ def test_batch_surrogate_trusted_runs(marl):
     with pytest.raises(marl.MarlError):
         b.set_surrogate(s, marl.SURR_CAPTURE)
     s.close()
+
+
+# Five runs of ~9,000 seeded cells each: together more cells than the batched
+# cell kernel's grid has lanes (2 resident blocks x 148 SMs x 128 = 37,888),
+# so the batch advances them by lane refill, while each single-run engine
+# (9,000 cells, one lane each) uses warp tickets.
+BIG_RUNS = [((96, 96, 48), seed, 3000, 1 << 15) for seed in (21, 22, 23, 24, 25)]
+
+
+def test_batch_lane_refill_matches_single_engines(marl):
+    p = marl.default_params()
+    ticks = 8
+    b = marl.Batch(BIG_RUNS, p)
+    total = sum(b.stats(r)["population"] for r in range(len(BIG_RUNS)))
+    assert total > 37_888, total
+    b.step(ticks)
+    for r, (dims, seed, seed_count, cap) in enumerate(BIG_RUNS):
+        e = marl.Engine(dims, p, rng_seed=seed, seed_count=seed_count, cell_capacity=cap)
+        e.step(ticks)
+        assert_run_equal(b, r, e)
+        e.close()
+
+
+def test_batch_surrogate_gated_zero_tolerance_under_lane_refill(marl):
+    """Gated at tolerance 0 through the lane-refill form of the batched loop
+    reproduces the plain batch bit for bit."""
+    p = marl.default_params()
+    s = captured_surrogate(marl, p, seed=9)
+    plain = marl.Batch(BIG_RUNS, p)
+    plain.step(6)
+    gated = marl.Batch(BIG_RUNS, p)
+    gated.step(2)
+    gated.set_surrogate(s, marl.SURR_GATED, 0.0)
+    gated.step(4)
+    c = gated.surrogate_counters()
+    assert c["cells"] > 37_888 and c["max_err"] == 0.0
+    for r in range(len(BIG_RUNS)):
+        assert plain.cells(r).tobytes() == gated.cells(r).tobytes(), r
+        assert np.array_equal(plain.field(r).view(np.uint32), gated.field(r).view(np.uint32)), r
+    gated.set_surrogate(None, marl.SURR_OFF)
+    s.close()
