@@ -85,8 +85,9 @@ def clustered_state(dims, frac, seed):
     return cells, field, light
 
 
-def make_ctx(marl, dims, cells, field, light):
+def make_ctx(marl, dims, cells, field, light, lanes=32):
     ctx = marl.Context(dims, marl.default_params(), cell_capacity=len(cells))
+    marl._check(marl.load().marl_ctx_set_cell_lanes(ctx.h, lanes), "marl_ctx_set_cell_lanes")
     ctx.upload_field(field)
     ctx.upload_light(light)
     ctx.upload_cells(cells)
@@ -178,6 +179,35 @@ def test_gated_zero_tolerance_is_the_plain_tick(marl):
     assert c["max_err"] == 0.0
     # the pre-pass is exact for every cell whose neighbourhood no earlier cell writes
     assert c["speculated"] >= independent_cells(cells, dims)
+    s.close()
+
+
+@pytest.mark.parametrize("mode", ["gated", "trusted"])
+def test_surrogate_modes_under_lane_refill(marl, mode):
+    """With one cell per warp ticket the grid has 1,184 lanes, fewer than the
+    cells, so the surrogate modes run through the lane-refill loop.  Gated at
+    tolerance 0 it equals the plain phase (run with warp tickets) bit for bit;
+    trusted accepts every speculated cell."""
+    dims = (40, 32, 24)
+    cells, field, light = clustered_state(dims, 0.3, 12)
+    assert len(cells) > 1184
+    s = prepared_surrogate(marl, dims, cells, field, light, seed=4)
+    plain = make_ctx(marl, dims, cells, field, light)
+    ev_plain = plain.cell_phase()
+    ctx = make_ctx(marl, dims, cells, field, light, lanes=1)
+    m = marl.SURR_GATED if mode == "gated" else marl.SURR_TRUSTED
+    marl.ctx_set_surrogate(ctx.h, s, m, 0.0)
+    ev = ctx.cell_phase()
+    c = marl.ctx_surrogate_counters(ctx.h)
+    assert c["cells"] == len(cells)
+    assert c["accepted"] + c["rejected"] == c["speculated"] <= c["cells"]
+    if mode == "gated":
+        assert c["max_err"] == 0.0
+        np.testing.assert_array_equal(ev, ev_plain)
+        np.testing.assert_array_equal(ctx.download_field(), plain.download_field())
+        assert ctx.download_cells().tobytes() == plain.download_cells().tobytes()
+    else:
+        assert c["rejected"] == 0 and c["accepted"] == c["speculated"] > 0
     s.close()
 
 
