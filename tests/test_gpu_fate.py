@@ -291,3 +291,25 @@ def test_batch_switches_fate_modes(marl):
         e.set_device_fate(False)
         e.step(10)
         assert_batch_run_equal(b, r, e)
+
+
+def test_device_fate_under_lane_refill(marl):
+    """Device fate with one cell per warp ticket: the grid has 1,184 lanes,
+    fewer than the ~3,000 seeded cells, so every tick's cell loop (reading its
+    cell count on the device) runs by lane refill.  It must equal the same
+    run with 32 cells per ticket (warp tickets) bit for bit."""
+    dims = (96, 96, 48)
+    p = marl.default_params()
+    runs = []
+    for lanes in (32, 1):
+        e = marl.Engine(dims, p, rng_seed=5, seed_count=1000, cell_capacity=1 << 15)
+        marl._check(e.lib.marl_ctx_set_cell_lanes(e.lib.marl_engine_ctx(e.h), lanes), "marl_ctx_set_cell_lanes")
+        e.set_device_fate(True)
+        e.step(12)
+        runs.append(e)
+    a, b = runs
+    assert a.stats()["population"] > 1184
+    for k in ("tick", "population", "total_divisions", "total_deaths"):
+        assert a.stats()[k] == b.stats()[k], k
+    assert a.cells().tobytes() == b.cells().tobytes()
+    np.testing.assert_array_equal(a.field().view(np.uint32), b.field().view(np.uint32))
