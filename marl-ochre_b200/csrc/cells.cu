@@ -651,10 +651,10 @@ __device__ __forceinline__ void cell_tick_loop_tickets(CellScratch& S, const Cel
 }
 
 // Lane refill: each warp keeps up to `lanes` cells in flight, one per lane,
-// and works in rounds: poll the dependencies of its staged cells, update the ready ones
-// together, then hand every lane that is free the next index from the ticket
-// counter (in lane order, so indices still go out in ascending order) and
-// stage its cell.  A cell whose dependency is still running holds only its
+// and works in rounds: poll the dependencies of its staged cells, update the
+// ready ones together, then hand every lane that is free the next index from
+// the ticket counter (in lane order, so indices still go out in ascending
+// order) and stage its cell.  A cell whose dependency is still running holds only its
 // own lane; the other lanes move on to new cells.  Staging writes only shared
 // memory (cp.async), and its copies are awaited at the start of the next
 // round, so an update never waits on another lane's loads.  The ticket request
