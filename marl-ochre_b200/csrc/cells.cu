@@ -35,9 +35,12 @@ namespace marl {
 __constant__ int c_face[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
 
 // ---------------------------------------------------------- schedule -----
-__device__ __forceinline__ void schedule_cell(const CellTable& t, const Grid g, const int32_t* __restrict__ cmap,
-                                              const uint32_t j) {
-    const uint32_t P = t.pos[j];
+// The empty-face bits of cell j at packed position P, and through each face
+// f its dependency (the largest cell index below j touching that voxel, or
+// -1), handed to put_dep(f, dep); returns the bits.
+template <class PutDep>
+__device__ __forceinline__ uint32_t schedule_of(const Grid g, const int32_t* __restrict__ cmap, const uint32_t P,
+                                                const uint32_t j, PutDep put_dep) {
     const int x = pos_x(P), y = pos_y(P), z = pos_z(P);
     uint32_t nb = 0;
 #pragma unroll
@@ -56,9 +59,14 @@ __device__ __forceinline__ void schedule_cell(const CellTable& t, const Grid g, 
                 }
             }
         }
-        t.dep[(size_t)f * t.cap + j] = dep;
+        put_dep(f, dep);
     }
-    t.nb[j] = nb;
+    return nb;
+}
+
+__device__ __forceinline__ void schedule_cell(const CellTable& t, const Grid g, const int32_t* __restrict__ cmap,
+                                              const uint32_t j) {
+    t.nb[j] = schedule_of(g, cmap, t.pos[j], j, [&](int f, int32_t dep) { t.dep[(size_t)f * t.cap + j] = dep; });
 }
 
 // n_dev (nullable): device-resident cell count, which then replaces n.
@@ -157,11 +165,15 @@ struct CellRunView {
     uint32_t epoch;
     const SurrView* sv;  // surrogate modes only
     float* act;          // receptor activations [8][cap], or null
+    const int32_t* cmap; // voxel -> cell map (for a schedule computed in the loop)
 };
 
 // Issues (and commits as one group) the asynchronous copies of cell j's table
 // entries into the lane's staging slots; cp_async_wait_all() completes them.
-__device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j) {
+// With schedule_here the empty-face bits and dependencies are computed from
+// the cell map instead of read from the table (no schedule kernel ran).
+__device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S, uint32_t j,
+                                           bool schedule_here = false) {
     const int tid = threadIdx.x;
     const CellTable& t = *v.t;
     const size_t cap = t.cap;
@@ -176,13 +188,18 @@ __device__ __forceinline__ void stage_cell(const CellRunView& v, CellScratch& S,
     cp_async16(&S.fate[tid], &t.fate[j]);
 #pragma unroll
     for (int k = 0; k < MARL_M_INT; ++k) cp_async4(&S.x[k][tid], &t.internal[k * cap + j]);
-    cp_async4(&S.hdr[0][tid], &t.nb[j]);
     cp_async4(&S.hdr[1][tid], &t.pos[j]);
     cp_async4(&S.hdr[2][tid], &t.state[j]);
     cp_async4(&S.hdr[3][tid], &t.age[j]);
-    // The schedule stores -1 for faces that are not empty in-grid voxels.
+    if (schedule_here) {
+        S.hdr[0][tid] = schedule_of(v.g, v.cmap, t.pos[j], j,
+                                    [&](int f, int32_t dep) { S.hdr[4 + f][tid] = (uint32_t)dep; });
+    } else {
+        cp_async4(&S.hdr[0][tid], &t.nb[j]);
+        // The schedule stores -1 for faces that are not empty in-grid voxels.
 #pragma unroll
-    for (int f = 0; f < 6; ++f) cp_async4(&S.hdr[4 + f][tid], &t.dep[(size_t)f * cap + j]);
+        for (int f = 0; f < 6; ++f) cp_async4(&S.hdr[4 + f][tid], &t.dep[(size_t)f * cap + j]);
+    }
     cp_async_commit();
 }
 
@@ -607,7 +624,7 @@ __device__ __forceinline__ void cell_tick_loop_tickets(CellScratch& S, const Cel
         uint32_t j = 0;
         if (pending) {
             resolve(gi, v, j);
-            stage_cell(v, S, j);
+            stage_cell(v, S, j, c.schedule_here != 0);
         }
         cp_async_wait_all();
         // Dependencies not yet seen finished (bit f: face f).  A poll loads
@@ -717,7 +734,7 @@ __device__ __forceinline__ void cell_tick_loop_refill(CellScratch& S, const Cell
                 if (next < total) {
                     gi = next;
                     resolve(gi, v, j);
-                    stage_cell(v, S, j);
+                    stage_cell(v, S, j, c.schedule_here != 0);
                     pending = true;
                     spins = 0;
                     remaining = kUnscanned;
@@ -748,7 +765,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick(const __grid_constan
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     const uint32_t total = a.n_dev ? *a.n_dev : a.n;
     cell_tick_loop<MODE>(S, a.k, total, a.ticket, a.err, a.lanes, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
-        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv, a.act};
+        v = CellRunView{&a.t, a.g, a.field, a.light, a.epoch, &a.sv, a.act, a.cmap};
         j = gi;
     });
 }
@@ -859,7 +876,7 @@ __global__ void __launch_bounds__(kTickThreads) k_cell_tick_batch(const RunDesc*
     CellScratch& S = *reinterpret_cast<CellScratch*>(tick_smem);
     cell_tick_loop<MODE>(S, c, batch_total(runs, n_runs), &bs->ticket, &bs->err, 32u, [&](uint32_t gi, CellRunView& v, uint32_t& j) {
         const RunDesc& R = runs[find_run(runs, n_runs, gi)];
-        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv, nullptr};
+        v = CellRunView{&R.t, R.g, R.field[parity], R.light, R.epoch, &R.sv, nullptr, R.cmap};
         j = gi - R.cell_base;
     });
 }
@@ -1249,6 +1266,21 @@ static cudaError_t launch_cell_tick_mode(const CellLaunch& a, int num_sms, cudaS
     const uint32_t blocks = blocks_needed < resident ? blocks_needed : resident;
     k_cell_tick<MODE><<<blocks, kTickThreads, kTickSmem, s>>>(a);
     return cudaGetLastError();
+}
+
+bool cell_tick_covers(uint32_t n, uint32_t lanes, int num_sms) {
+    static std::atomic<int> setup[kSetupDevices];
+    int per_sm = 1;
+    if (setup_once(setup, &per_sm, [](int* v) {
+            cudaError_t r = cudaFuncSetAttribute(k_cell_tick<kModePlain>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 kTickSmem);
+            if (r != cudaSuccess) return r;
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, k_cell_tick<kModePlain>, kTickThreads, kTickSmem);
+            if (*v < 1) *v = 1;
+            return r;
+        }) != cudaSuccess)
+        return false;
+    return (uint64_t)n <= (uint64_t)per_sm * (uint64_t)num_sms * (kTickThreads / 32) * lanes;
 }
 
 cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s) {

@@ -80,6 +80,7 @@ struct CellConsts {
     float base_division_prep, prep_maintenance_multiplier, rush_penalty_rate;
     uint32_t wait_limit;  // polls of a dependency flag before the wait gives up (kErrTimeoutDeps)
     float hill_lo, hill_hi;  // receptor Hill exponent clamp (receptor activations)
+    uint32_t schedule_here;  // the cell loop computes the schedule itself (no schedule kernel ran)
 };
 
 struct Grid {

@@ -94,6 +94,7 @@ void derive_consts(const marl_sim_params& p, FieldConsts* fk, CellConsts* ck) {
     ck->prep_maintenance_multiplier = p.prep_maintenance_multiplier;
     ck->rush_penalty_rate = p.rush_penalty_rate;
     ck->wait_limit = kFlagSpinLimit;
+    ck->schedule_here = 0;
     ck->hill_lo = p.hill_exponent_clamp_low;
     ck->hill_hi = p.hill_exponent_clamp_high;
 }
@@ -251,7 +252,15 @@ marl_status enqueue_cell_phase(marl_ctx* c) {
     if (c->n == 0 && !c->n_on_device) return MARL_OK;
     c->c4_valid = false;  // the scatter writes every species
     CellLaunch a = cell_launch(c);
-    if (c->schedule_dirty) {
+    // When every cell gets a lane at once and nothing else needs the table's
+    // schedule this phase (no surrogate, no dependency hold, population on
+    // the host), the cell kernel computes each cell's schedule while staging
+    // it, and the schedule kernel is skipped.  The table's schedule is then
+    // left stale (schedule_dirty stays set) for any later phase that reads it.
+    const bool schedule_here = (!c->surr || c->surr_mode == MARL_SURR_OFF) && c->hold_cell < 0 &&
+                               !c->n_on_device && cell_tick_covers(c->n, c->cell_lanes, c->num_sms);
+    a.k.schedule_here = schedule_here ? 1u : 0u;
+    if (c->schedule_dirty && !schedule_here) {
         CK(launch_cell_schedule(a, c->stream));
         c->schedule_dirty = false;
         ++c->launches;

@@ -161,6 +161,9 @@ cudaError_t launch_cell_schedule(const CellLaunch& a, cudaStream_t s);
 cudaError_t launch_hold_dependency(const CellTable& t, uint32_t cell, int face, uint32_t slot, uint32_t* err,
                                    cudaStream_t s);
 cudaError_t launch_cell_tick(const CellLaunch& a, int num_sms, cudaStream_t s);
+// Whether the plain cell kernel's grid gives each of n cells its own lane at
+// once (warp tickets); then the kernel can compute the schedule itself.
+bool cell_tick_covers(uint32_t n, uint32_t lanes, int num_sms);
 // Surrogate pre-pass: every cell's gather and transport on the current field
 // (as the cell loop would compute them if no earlier cell had written its
 // neighbourhood): xt [16][cap] and the standardised BF16 features X [cap][128].
