@@ -1163,12 +1163,6 @@ __device__ __forceinline__ void halve_one(const CellTable& t, uint32_t p, uint32
     v = v * 0.5f;
 }
 
-__global__ void k_halve(CellTable t, const uint32_t* __restrict__ idx, uint32_t count) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count * MARL_M_INT) return;
-    halve_one(t, idx[i / MARL_M_INT], i % MARL_M_INT);
-}
-
 __global__ void k_halve_batch(const RunDesc* __restrict__ runs, const uint2* __restrict__ items, uint32_t count) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count * MARL_M_INT) return;
@@ -1185,17 +1179,27 @@ __device__ __forceinline__ void clear_dead_one(const CellTable& t, const Grid g,
     mask[row * mask_pitch(g.X) + pos_x(P)] = 0;
 }
 
-__global__ void k_clear_dead(CellTable t, const uint32_t* __restrict__ idx, uint32_t count, Grid g,
-                             int32_t* __restrict__ cmap, uint8_t* __restrict__ mask) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) clear_dead_one(t, g, cmap, mask, idx[i]);
-}
-
 __global__ void k_clear_dead_batch(const RunDesc* __restrict__ runs, const uint2* __restrict__ items, uint32_t count) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const RunDesc& R = runs[items[i].x];
     clear_dead_one(R.t, R.g, R.cmap, R.mask, items[i].y);
+}
+
+// Halving and dead-cell clearing of one edit list in one launch: threads
+// [0, 16 n_halve) halve, the next n_dead clear.  A cell of the change list
+// either divides or dies, so the two touch different cells; both must finish
+// before the moves (a moved parent is copied halved, a dead slot's position
+// is read before a move overwrites it).
+__global__ void k_halve_clear(CellTable t, const uint32_t* __restrict__ halve_idx, uint32_t n_halve,
+                              const uint32_t* __restrict__ dead_idx, uint32_t n_dead, Grid g,
+                              int32_t* __restrict__ cmap, uint8_t* __restrict__ mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nh = n_halve * MARL_M_INT;
+    if (i < nh)
+        halve_one(t, halve_idx[i / MARL_M_INT], i % MARL_M_INT);
+    else if (i - nh < n_dead)
+        clear_dead_one(t, g, cmap, mask, dead_idx[i - nh]);
 }
 
 // swap_remove moves (lib.rs:258-267), one warp per move (move_one, table_ops.cuh).
@@ -1353,16 +1357,12 @@ cudaError_t launch_cells_to_records(const CellTable& t, uint32_t n, marl_cell* r
     return cudaGetLastError();
 }
 
-cudaError_t launch_halve(const CellTable& t, const uint32_t* idx, uint32_t count, cudaStream_t s) {
-    if (count == 0) return cudaSuccess;
-    k_halve<<<blocks_for((size_t)count * MARL_M_INT, 256), 256, 0, s>>>(t, idx, count);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_clear_dead(const CellTable& t, const uint32_t* idx, uint32_t count, const Grid& g, int32_t* cmap,
-                              uint8_t* mask, cudaStream_t s) {
-    if (count == 0) return cudaSuccess;
-    k_clear_dead<<<blocks_for(count, 256), 256, 0, s>>>(t, idx, count, g, cmap, mask);
+cudaError_t launch_halve_clear(const CellTable& t, const uint32_t* halve_idx, uint32_t n_halve,
+                               const uint32_t* dead_idx, uint32_t n_dead, const Grid& g, int32_t* cmap, uint8_t* mask,
+                               cudaStream_t s) {
+    const size_t items = (size_t)n_halve * MARL_M_INT + n_dead;
+    if (items == 0) return cudaSuccess;
+    k_halve_clear<<<blocks_for(items, 256), 256, 0, s>>>(t, halve_idx, n_halve, dead_idx, n_dead, g, cmap, mask);
     return cudaGetLastError();
 }
 

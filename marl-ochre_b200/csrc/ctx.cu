@@ -908,13 +908,12 @@ marl_status marl_apply_edits(marl_ctx* c, const marl_edit_list* e) {
     const uint32_t* dd = (const uint32_t*)(d + b_halve);
     const uint32_t* dmd = (const uint32_t*)(d + b_halve + b_deaths);
     const uint32_t* dms = (const uint32_t*)(d + b_halve + b_deaths + b_mv);
-    CK(launch_halve(c->t, dh, e->n_halve, c->stream));
-    CK(launch_clear_dead(c->t, dd, e->n_deaths, c->g, c->cmap, c->mask, c->stream));
+    CK(launch_halve_clear(c->t, dh, e->n_halve, dd, e->n_deaths, c->g, c->cmap, c->mask, c->stream));
     CK(launch_moves(c->t, dmd, dms, e->n_moves, c->g, c->cmap, c->stream));
     CK(launch_cells_from_records((const marl_cell*)(d + off_births), e->n_births, e->n_after_deaths, c->t, c->g,
                                  c->cmap, c->mask, &c->d_hdr->err, c->stream));
     span_end(c, span);
-    c->launches += (e->n_halve > 0) + (e->n_deaths > 0) + (e->n_moves > 0) + (e->n_births > 0);
+    c->launches += (e->n_halve > 0 || e->n_deaths > 0) + (e->n_moves > 0) + (e->n_births > 0);
     c->n = e->n_after_deaths + e->n_births;
     if (e->n_deaths || e->n_births || e->n_moves) c->schedule_dirty = true;
     return MARL_OK;

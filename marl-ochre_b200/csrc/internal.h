@@ -182,9 +182,11 @@ cudaError_t launch_compact_events(const CellTable& t, uint32_t n, uint32_t* bloc
 cudaError_t launch_cells_from_records(const marl_cell* rec, uint32_t count, uint32_t base, CellTable t, const Grid& g,
                                       int32_t* cmap, uint8_t* mask, uint32_t* err, cudaStream_t s);
 cudaError_t launch_cells_to_records(const CellTable& t, uint32_t n, marl_cell* rec, cudaStream_t s);
-cudaError_t launch_halve(const CellTable& t, const uint32_t* idx, uint32_t count, cudaStream_t s);
-cudaError_t launch_clear_dead(const CellTable& t, const uint32_t* idx, uint32_t count, const Grid& g, int32_t* cmap,
-                              uint8_t* mask, cudaStream_t s);
+// Halving of the parents and clearing of the dead cells of one edit list, in
+// one launch.
+cudaError_t launch_halve_clear(const CellTable& t, const uint32_t* halve_idx, uint32_t n_halve,
+                               const uint32_t* dead_idx, uint32_t n_dead, const Grid& g, int32_t* cmap, uint8_t* mask,
+                               cudaStream_t s);
 cudaError_t launch_moves(CellTable t, const uint32_t* dst, const uint32_t* src, uint32_t count, const Grid& g,
                          int32_t* cmap, cudaStream_t s);
 cudaError_t launch_rebuild_maps(const CellTable& t, uint32_t n, const Grid& g, int32_t* cmap, uint8_t* mask,
